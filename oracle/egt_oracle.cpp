@@ -1,0 +1,827 @@
+// CPU oracle for the grid-kNN -> EGT -> Taubin -> normals path.
+//
+// ORACLE / TEST INFRASTRUCTURE.  This is a plain C++17/OpenMP restatement of the
+// reference implementation (agalex1974/MultiGPUEGTSmoothing) used only by the
+// tests, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg, as the
+// checker.  The product never links it.  Every function cites the reference
+// file:line it follows.  Parity of this oracle with the reference itself is
+// pinned by the golden fixtures in tests/golden (generated by running the
+// unmodified reference, see tests/golden/make_golden.py).
+//
+// Conventions (all arrays are caller-owned):
+//   xyz        original points, AoS float32 [n*3]
+//   pos        normalised points in cell-sorted order, SoA float32 [3*n]
+//   perm       sorted slot -> original index, int32 [n]
+//   lists      sorted-space neighbour lists, int32 [n*k], -1 padded
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <queue>
+#include <set>
+#include <vector>
+#include <omp.h>
+
+#include "fp_shapes.h"
+
+using namespace fpshape;
+
+namespace {
+
+constexpr float kEps = 1e-6f;          // GridStructure eps (main.cpp:108)
+constexpr int kBuckets = 1024;         // level-0 bucket count (main.cpp:108)
+constexpr int kMaxPointsInCube = 100000;  // MAX_PNTS_IN_CUBE default (GridKNNCuda.cu:652)
+constexpr int kLevels = 8;             // levels 0..7 (B = 1024..8) are searched
+
+// Reference GridKNNCuda.cu:1042-1071 (InitStructure): one scalar cube for all axes.
+void cube_extents(const float* xyz, int n, float& mn, float& mx) {
+    float lo[3] = {1e8f, 1e8f, 1e8f}, hi[3] = {-1e8f, -1e8f, -1e8f};
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < 3; d++) {
+            lo[d] = std::min(lo[d], xyz[3 * (size_t)i + d]);
+            hi[d] = std::max(hi[d], xyz[3 * (size_t)i + d]);
+        }
+    for (int d = 0; d < 3; d++) { lo[d] = lo[d] - 1e-6f; hi[d] = hi[d] + 1e-6f; }
+    mn = std::min(std::min(lo[0], lo[1]), lo[2]);
+    mx = std::max(std::max(hi[0], hi[1]), hi[2]);
+}
+
+// Cell coordinate (GridKNNCuda.cu:74-88, :649-653): (int)((x-a)/(b-a)*B).
+inline int cell_coord(float x, float a, float b, int B) {
+    return (int)((x - a) / (b - a) * (float)B);
+}
+
+struct Grid {
+    int n = 0;
+    float mn = 0, mx = 0;          // normalisation cube
+    float a = -kEps, b = 0;        // unit-cube bounds with eps
+    std::vector<int> perm;         // sorted slot -> original
+    std::vector<float> x, y, z;    // normalised, sorted
+    std::vector<int> cx, cy, cz;   // level-0 cell coords per sorted point
+    struct Level {
+        int B = 0;
+        std::vector<int> keys;     // unique occupied cell keys, ascending
+        std::vector<int> start;    // start offset of each cell in `order`
+        std::vector<int> order;    // sorted indices grouped by cell, ascending inside a cell
+    } lv[kLevels];
+};
+
+// InitStructure (GridKNNCuda.cu:1023-1133): normalise, level-0 key, stable sort, gather.
+void build_grid(const float* xyz, int n, Grid& g, int levels) {
+    g.n = n;
+    cube_extents(xyz, n, g.mn, g.mx);
+    g.b = (float)(1.0 + (double)kEps);
+    const float d = g.mx - g.mn;
+    std::vector<float> nx(n), ny(n), nz(n);
+    std::vector<int> key(n);
+    for (int i = 0; i < n; i++) {
+        nx[i] = (xyz[3 * (size_t)i] - g.mn) / d;
+        ny[i] = (xyz[3 * (size_t)i + 1] - g.mn) / d;
+        nz[i] = (xyz[3 * (size_t)i + 2] - g.mn) / d;
+        int xi = cell_coord(nx[i], g.a, g.b, kBuckets);
+        int yi = cell_coord(ny[i], g.a, g.b, kBuckets);
+        int zi = cell_coord(nz[i], g.a, g.b, kBuckets);
+        key[i] = xi + yi * kBuckets + zi * kBuckets * kBuckets;
+    }
+    g.perm.resize(n);
+    std::iota(g.perm.begin(), g.perm.end(), 0);
+    std::stable_sort(g.perm.begin(), g.perm.end(), [&](int p, int q) { return key[p] < key[q]; });
+    g.x.resize(n); g.y.resize(n); g.z.resize(n);
+    g.cx.resize(n); g.cy.resize(n); g.cz.resize(n);
+    for (int s = 0; s < n; s++) {
+        int o = g.perm[s];
+        g.x[s] = nx[o]; g.y[s] = ny[o]; g.z[s] = nz[o];
+        g.cx[s] = cell_coord(g.x[s], g.a, g.b, kBuckets);
+        g.cy[s] = cell_coord(g.y[s], g.a, g.b, kBuckets);
+        g.cz[s] = cell_coord(g.z[s], g.a, g.b, kBuckets);
+    }
+    // Levels (getBuckets / InitializeLevel, GridKNNCuda.cu:898-946): a stable sort
+    // of the sorted indices by the level-L key.  Level-L cell = level-0 cell >> L
+    // because u*B_L = (u*1024)/2^L exactly in floating point.
+    for (int L = 0; L < levels; L++) {
+        auto& lv = g.lv[L];
+        lv.B = kBuckets >> L;
+        std::vector<int> kL(n);
+        for (int s = 0; s < n; s++)
+            kL[s] = (g.cx[s] >> L) + (g.cy[s] >> L) * lv.B + (g.cz[s] >> L) * lv.B * lv.B;
+        lv.order.resize(n);
+        std::iota(lv.order.begin(), lv.order.end(), 0);
+        std::stable_sort(lv.order.begin(), lv.order.end(), [&](int p, int q) { return kL[p] < kL[q]; });
+        lv.keys.clear(); lv.start.clear();
+        for (int i = 0; i < n; i++) {
+            int kk = kL[lv.order[i]];
+            if (i == 0 || kk != lv.keys.back()) { lv.keys.push_back(kk); lv.start.push_back(i); }
+        }
+        lv.start.push_back(n);
+    }
+}
+
+// FindPosition (GridKNNCuda.cu:126-143): binary search that returns the slot of
+// an equal element if one is hit, otherwise the insertion point.
+inline int find_position(const float* a, float x, int low, int high) {
+    while (low <= high) {
+        int mid = low + (high - low) / 2;
+        if (a[mid] == x) return mid;
+        if (a[mid] < x) low = mid + 1;
+        else high = mid - 1;
+    }
+    return low + (high - low) / 2;
+}
+
+// newNeighborSearch::appendDistanceGrid (GridKNNCuda.cu:311-339).
+inline void append(float* dist, int* idx, int k, int& counter, float d, int p) {
+    if (!(d < dist[k - 1])) return;
+    for (int i = 0; i < counter; i++)
+        if (idx[i] == p) return;
+    int pos = find_position(dist, d, 0, counter - 1);
+    if (counter == k) counter--;
+    for (int i = counter - 1; i >= pos; i--) { dist[i + 1] = dist[i]; idx[i + 1] = idx[i]; }
+    dist[pos] = d; idx[pos] = p;
+    counter++;
+}
+
+// Shell cell order of GRIDCUDAKNNSELF_COMPACT for offset 1 (GridKNNCuda.cu:2480-2551).
+const int kShell[26][3] = {
+    {0, 0, -1}, {0, 0, 1},
+    {0, -1, 0}, {0, 1, 0},
+    {-1, 0, 0}, {1, 0, 0},
+    {-1, -1, 0}, {-1, 1, 0}, {1, -1, 0}, {1, 1, 0},
+    {-1, 0, -1}, {-1, 0, 1}, {1, 0, -1}, {1, 0, 1},
+    {0, -1, -1}, {0, -1, 1}, {0, 1, -1}, {0, 1, 1},
+    {-1, -1, -1}, {-1, -1, 1}, {-1, 1, -1}, {-1, 1, 1}, {1, -1, -1}, {1, -1, 1}, {1, 1, -1}, {1, 1, 1},
+};
+
+struct KnnStats { long long visited_points = 0; int max_level = 0; };
+
+// One query of GRIDCUDAKNNSELF_COMPACT (GridKNNCuda.cu:2322-2586) with the
+// kernel body construct_neighbors_self_compact (GridKNNCuda.cu:647-743).
+// Returns the level reached (0..7, or 8 when the query ran out of levels).
+int knn_query(const Grid& g, int q, int k, float thres, float* dist, int* idx, int& counter,
+              bool& invalid, long long& visited) {
+    for (int i = 0; i < k; i++) { dist[i] = 1e10f; idx[i] = -1; }
+    counter = 0;
+    invalid = false;
+    const float xq = g.x[q], yq = g.y[q], zq = g.z[q];
+    const float xmin = g.a;
+
+    auto visit = [&](int L, int cx, int cy, int cz) {
+        const auto& lv = g.lv[L];
+        if (cx < 0 || cx >= lv.B || cy < 0 || cy >= lv.B || cz < 0 || cz >= lv.B) return;
+        int key = cx + cy * lv.B + cz * lv.B * lv.B;
+        auto it = std::lower_bound(lv.keys.begin(), lv.keys.end(), key);
+        if (it == lv.keys.end() || *it != key) return;
+        if (invalid) return;
+        size_t c = it - lv.keys.begin();
+        int s0 = lv.start[c], s1 = lv.start[c + 1];
+        if (s1 - s0 >= kMaxPointsInCube) { invalid = true; return; }
+        for (int j = s0; j < s1; j++) {
+            int p = lv.order[j];
+            if (p == q) continue;
+            float d = dist3(xq, yq, zq, g.x[p], g.y[p], g.z[p]);
+            visited++;
+            if (d <= thres) append(dist, idx, k, counter, d, p);
+        }
+    };
+    // Continue decision on the last cube of a shell (GridKNNCuda.cu:694-741).
+    auto decide = [&](int L, int o) -> bool {
+        if (invalid) return false;
+        const int B = g.lv[L].B;
+        const float h = (g.b - g.a) / (float)B;
+        const int xi = g.cx[q] >> L, yi = g.cy[q] >> L, zi = g.cz[q] >> L;
+        const float c[3] = {xq, yq, zq};
+        const int ci[3] = {xi, yi, zi};
+        if (counter < k) {
+            const float st = std::sqrt(thres);
+            for (int d = 0; d < 3; d++) {
+                if (ci[d] - o >= 0 && st > face_lo(c[d], xmin, (float)(ci[d] - o), h)) return true;
+                if (ci[d] + o + 1 <= B && st > face_hi(c[d], xmin, (float)(ci[d] + o + 1), h)) return true;
+            }
+            return false;
+        }
+        const float r = std::sqrt(dist[k - 1]);
+        bool more = false;
+        for (int d = 0; d < 3; d++) {
+            if (ci[d] - o >= 0 && r >= face_lo(c[d], xmin, (float)(ci[d] - o), h)) more = true;
+            if (ci[d] + o + 1 <= B && r >= face_hi(c[d], xmin, (float)(ci[d] + o + 1), h)) more = true;
+        }
+        return more;
+    };
+
+    visit(0, g.cx[q], g.cy[q], g.cz[q]);
+    bool cont = decide(0, 0);
+    int L = 0;
+    int reached = 0;
+    while (cont) {
+        reached = L;
+        const int xi = g.cx[q] >> L, yi = g.cy[q] >> L, zi = g.cz[q] >> L;
+        for (int s = 0; s < 26; s++) visit(L, xi + kShell[s][0], yi + kShell[s][1], zi + kShell[s][2]);
+        cont = decide(L, 1);
+        if (L == kLevels - 1) break;
+        L++;
+    }
+    // A query still searching after the B=8 ring is invalid (GridKNNCuda.cu:2572-2586).
+    if (cont) { invalid = true; reached = kLevels; }
+    if (invalid)
+        for (int i = 0; i < k; i++) idx[i] = -1;
+    return reached;
+}
+
+// EGT predicate isEllipicGabrielNeighbor_GKNN (EGT_CUDA.cu:136-170) with its
+// helpers (EGT_CUDA.cu:34-134).
+inline void normalize3(float& x, float& y, float& z) {
+    float nrm = std::sqrt(sq3(x, y, z));
+    x /= nrm; y /= nrm; z /= nrm;
+}
+
+bool egt_keep(const float* X, const float* Y, const float* Z, const int* row, int j,
+              float x, float y, float z, float alpha) {
+    const int nb = row[j];
+    float xi = X[nb], yi = Y[nb], zi = Z[nb];
+    float xo = 0.5f * (xi + x), yo = 0.5f * (yi + y), zo = 0.5f * (zi + z);
+    float d = std::sqrt(dist3(xi, yi, zi, x, y, z)) / 2.0f;
+    if ((double)d < 1e-6) return true;
+    float ax = xi - x, ay = yi - y, az = zi - z;
+    if ((double)std::sqrt(sq3(ax, ay, az)) < 1e-6) return true;
+    normalize3(ax, ay, az);
+    // perpendicular (EGT_CUDA.cu:61-95)
+    float mxv = std::fabs(ax);
+    int ci = 0;
+    if (mxv < std::fabs(ay)) { ci = 1; mxv = std::fabs(ay); }
+    if (mxv < std::fabs(az)) ci = 2;
+    float px = 1.0f, py = 1.0f, pz = 1.0f;
+    if (ci == 0) px = (-ay * py - az * pz) / ax;
+    else if (ci == 1) py = (-ax * px - az * pz) / ay;
+    else pz = (-ax * px - ay * py) / az;
+    normalize3(px, py, pz);
+    // third axis = x-axis cross perpendicular (EGT_CUDA.cu:97-104, 126-127)
+    float qx = cross1(ay, pz, py, az);
+    float qy = cross1(px, az, ax, pz);
+    float qz = cross1(ax, py, px, ay);
+    normalize3(qx, qy, qz);
+    // translation: A * o with a14 = a24 = a34 = 0 (EGT_CUDA.cu:128-133)
+    float tx = affine(ax, ay, az, 0.0f, xo, yo, zo);
+    float ty = affine(px, py, pz, 0.0f, xo, yo, zo);
+    float tz = affine(qx, qy, qz, 0.0f, xo, yo, zo);
+    tx = -tx; ty = -ty; tz = -tz;
+    const float aa = alpha * alpha;
+    const float dd = d * d;
+    for (int jj = 0; jj < j; jj++) {
+        int m = row[jj];
+        if (m < 0) continue;
+        float ux = X[m], uy = Y[m], uz = Z[m];
+        float lx = affine(ax, ay, az, tx, ux, uy, uz);
+        float ly = affine(px, py, pz, ty, ux, uy, uz);
+        float lz = affine(qx, qy, qz, tz, ux, uy, uz);
+        if (ellipsoid(lx, ly, lz, aa) < dd) return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Symmetric 3x3 eigensolver: the iterative Householder + Givens algorithm of
+// D. Eberly ("A Robust Eigensolver for 3x3 Symmetric Matrices", Geometric
+// Tools), as used by the reference (EigenSolver.cuh:124-392, sorted by
+// SortEigenstuff EigenSolver.cuh:29-122).  T = float mirrors the reference's
+// rounding shapes; T = double is the FP64 oracle.
+template <typename T> struct Fp;
+template <> struct Fp<float> {
+    static float lin_add(float c, float a, float s, float b) { return lin2_add(c, a, s, b); }
+    static float lin_sub(float s, float a, float c, float b) { return lin2_sub(s, a, c, b); }
+    static float hyp2(float u, float v) { return sq2(u, v); }
+    static float sqrtv(float v) { return std::sqrt(v); }
+    static int alpha() { return 149; }
+};
+template <> struct Fp<double> {
+    static double lin_add(double c, double a, double s, double b) { return c * a + s * b; }
+    static double lin_sub(double s, double a, double c, double b) { return s * a - c * b; }
+    static double hyp2(double u, double v) { return u * u + v * v; }
+    static double sqrtv(double v) { return std::sqrt(v); }
+    static int alpha() { return 1074; }
+};
+
+template <typename T>
+void cos_sin(T u, T v, T& c, T& s) {  // GetCosSin (EigenSolver.cuh:353-373)
+    T len = Fp<T>::sqrtv(Fp<T>::hyp2(u, v));
+    if (len > T(0)) {
+        c = u / len; s = v / len;
+        if (c > T(0)) { c = -c; s = -s; }
+    } else { c = T(-1); s = T(0); }
+}
+
+template <typename T>
+bool converged(T d0, T d1, T sd) {  // Converged, aggressive = false (EigenSolver.cuh:375-391)
+    T sum = std::fabs(d0) + std::fabs(d1);
+    return sum + std::fabs(sd) == sum;
+}
+
+template <typename T>
+void eigen3(T a00, T a01, T a02, T a11, T a12, T a22, T eval[3], T evec[3][3]) {
+    using F = Fp<T>;
+    const T half = T(0.5), one = T(1);
+    bool isRotation = false;
+    T c = 0, s = 0;
+    cos_sin<T>(a12, -a02, c, s);
+    T term0 = F::lin_add(c, a00, s, a01);
+    T term1 = F::lin_add(c, a01, s, a11);
+    T term2 = F::lin_sub(s, a00, c, a01);
+    T term3 = F::lin_sub(s, a01, c, a11);
+    T b00 = F::lin_add(c, term0, s, term1);
+    T b01 = F::lin_sub(s, term0, c, term1);
+    T b11 = F::lin_sub(s, term2, c, term3);
+    T b12 = F::lin_sub(s, a02, c, a12);
+    T b22 = a22;
+    T Q[3][3] = {{c, s, 0}, {s, -c, 0}, {0, 0, 1}};
+    int power = 0;
+    T c2 = 0, s2 = 0;
+    if (std::fabs(b12) <= std::fabs(b01)) {
+        std::frexp(b12, &power);
+        int imax = 2 * (power + F::alpha() + 1);
+        for (int i = 0; i < imax; ++i) {
+            cos_sin<T>(half * (b00 - b11), b01, c2, s2);
+            s = F::sqrtv(half * (one - c2));
+            c = half * s2 / s;
+            for (int r = 0; r < 3; ++r) {
+                T t0 = F::lin_add(c, Q[r][0], s, Q[r][1]);
+                T t1 = Q[r][2];
+                T t2 = F::lin_sub(c, Q[r][1], s, Q[r][0]);
+                Q[r][0] = t0; Q[r][1] = t1; Q[r][2] = t2;
+            }
+            isRotation = !isRotation;
+            term0 = F::lin_add(c, b00, s, b01);
+            term1 = F::lin_add(c, b01, s, b11);
+            term2 = F::lin_sub(s, b00, c, b01);
+            term3 = F::lin_sub(s, b01, c, b11);
+            b00 = F::lin_add(c, term0, s, term1);
+            b01 = s * b12;
+            b11 = b22;
+            b12 = c * b12;
+            b22 = F::lin_sub(s, term2, c, term3);
+            if (converged<T>(b00, b11, b01)) {
+                cos_sin<T>(half * (b00 - b11), b01, c2, s2);
+                s = F::sqrtv(half * (one - c2));
+                c = half * s2 / s;
+                for (int r = 0; r < 3; ++r) {
+                    T t0 = F::lin_add(c, Q[r][0], s, Q[r][1]);
+                    T t1 = F::lin_sub(s, Q[r][0], c, Q[r][1]);
+                    Q[r][0] = t0; Q[r][1] = t1;
+                }
+                isRotation = !isRotation;
+                term0 = F::lin_add(c, b00, s, b01);
+                term1 = F::lin_add(c, b01, s, b11);
+                term2 = F::lin_sub(s, b00, c, b01);
+                term3 = F::lin_sub(s, b01, c, b11);
+                b00 = F::lin_add(c, term0, s, term1);
+                b11 = F::lin_sub(s, term2, c, term3);
+                break;
+            }
+        }
+    } else {
+        std::frexp(b01, &power);
+        int imax = 2 * (power + F::alpha() + 1);
+        for (int i = 0; i < imax; ++i) {
+            cos_sin<T>(half * (b11 - b22), b12, c2, s2);
+            s = F::sqrtv(half * (one - c2));
+            c = half * s2 / s;
+            for (int r = 0; r < 3; ++r) {
+                T t0 = F::lin_add(c, Q[r][1], s, Q[r][2]);
+                T t1 = Q[r][0];
+                T t2 = F::lin_sub(c, Q[r][2], s, Q[r][1]);
+                Q[r][0] = t0; Q[r][1] = t1; Q[r][2] = t2;
+            }
+            isRotation = !isRotation;
+            term0 = F::lin_add(c, b11, s, b12);
+            term1 = F::lin_add(c, b12, s, b22);
+            term2 = F::lin_sub(s, b11, c, b12);
+            term3 = F::lin_sub(s, b12, c, b22);
+            b22 = F::lin_sub(s, term2, c, term3);
+            b12 = -s * b01;
+            b11 = b00;
+            b01 = c * b01;
+            b00 = F::lin_add(c, term0, s, term1);
+            if (converged<T>(b11, b22, b12)) {
+                cos_sin<T>(half * (b11 - b22), b12, c2, s2);
+                s = F::sqrtv(half * (one - c2));
+                c = half * s2 / s;
+                for (int r = 0; r < 3; ++r) {
+                    T t0 = F::lin_add(c, Q[r][1], s, Q[r][2]);
+                    T t1 = F::lin_sub(s, Q[r][1], c, Q[r][2]);
+                    Q[r][1] = t0; Q[r][2] = t1;
+                }
+                isRotation = !isRotation;
+                term0 = F::lin_add(c, b11, s, b12);
+                term1 = F::lin_add(c, b12, s, b22);
+                term2 = F::lin_sub(s, b11, c, b12);
+                term3 = F::lin_sub(s, b12, c, b22);
+                b11 = F::lin_add(c, term0, s, term1);
+                b22 = F::lin_sub(s, term2, c, term3);
+                break;
+            }
+        }
+    }
+    T ev[3] = {b00, b11, b22};
+    T vec[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int col = 0; col < 3; ++col) vec[r][col] = Q[col][r];
+    // SortEigenstuff, sortType = +1 (increasing) and right-handed basis.
+    int index[3];
+    if (ev[0] < ev[1]) {
+        if (ev[2] < ev[0]) { index[0] = 2; index[1] = 0; index[2] = 1; }
+        else if (ev[2] < ev[1]) { index[0] = 0; index[1] = 2; index[2] = 1; isRotation = !isRotation; }
+        else { index[0] = 0; index[1] = 1; index[2] = 2; }
+    } else {
+        if (ev[2] < ev[1]) { index[0] = 2; index[1] = 1; index[2] = 0; isRotation = !isRotation; }
+        else if (ev[2] < ev[0]) { index[0] = 1; index[1] = 2; index[2] = 0; }
+        else { index[0] = 1; index[1] = 0; index[2] = 2; isRotation = !isRotation; }
+    }
+    for (int j = 0; j < 3; ++j) {
+        eval[j] = ev[index[j]];
+        for (int col = 0; col < 3; ++col) evec[j][col] = vec[index[j]][col];
+    }
+    if (!isRotation)
+        for (int col = 0; col < 3; ++col) evec[2][col] = -evec[2][col];
+}
+
+// calculateNormal (Normal_CUDA.cu:87-144), float or double arithmetic.
+template <typename T>
+void normal_of(const float* X, const float* Y, const float* Z, const int* row, int k, int i, T out[3]) {
+    T sx = X[i], sy = Y[i], sz = Z[i];
+    int cnt = 1;
+    for (int j = 0; j < k; j++) {
+        int m = row[j];
+        if (m >= 0) { sx += X[m]; sy += Y[m]; sz += Z[m]; cnt++; }
+    }
+    T cxm = sx / (T)cnt, cym = sy / (T)cnt, czm = sz / (T)cnt;
+    T c00 = 0, c01 = 0, c02 = 0, c11 = 0, c12 = 0, c22 = 0;
+    for (int j = 0; j < k; j++) {
+        int m = row[j];
+        if (m < 0) continue;
+        T dx = X[m] - cxm, dy = Y[m] - cym, dz = Z[m] - czm;
+        if constexpr (sizeof(T) == 4) {
+            c00 = cov_acc(c00, dx, dx); c01 = cov_acc(c01, dx, dy); c02 = cov_acc(c02, dx, dz);
+            c11 = cov_acc(c11, dy, dy); c12 = cov_acc(c12, dy, dz); c22 = cov_acc(c22, dz, dz);
+        } else {
+            c00 += dx * dx; c01 += dx * dy; c02 += dx * dz; c11 += dy * dy; c12 += dy * dz; c22 += dz * dz;
+        }
+    }
+    T ev[3], vec[3][3];
+    eigen3<T>(c00, c01, c02, c11, c12, c22, ev, vec);
+    T nx = vec[0][0], ny = vec[0][1], nz = vec[0][2];
+    T nrm;
+    if constexpr (sizeof(T) == 4) nrm = std::sqrt(sq3(nx, ny, nz));
+    else nrm = std::sqrt(nx * nx + ny * ny + nz * nz);
+    out[0] = nx / nrm; out[1] = ny / nrm; out[2] = nz / nrm;
+}
+
+struct DSU {
+    std::vector<int> p;
+    explicit DSU(int n) : p(n) { std::iota(p.begin(), p.end(), 0); }
+    int find(int a) { while (p[a] != a) { p[a] = p[p[a]]; a = p[a]; } return a; }
+    bool unite(int a, int b) { a = find(a); b = find(b); if (a == b) return false; p[a] = b; return true; }
+};
+
+}  // namespace
+
+extern "C" {
+
+int orc_num_threads() { return omp_get_max_threads(); }
+
+// Normalisation cube of InitStructure (GridKNNCuda.cu:1042-1071): ext = {min, max}.
+void orc_extents(const float* xyz, int n, float* ext) { cube_extents(xyz, n, ext[0], ext[1]); }
+
+// Grid kNN of the reference (GridStructure + GRIDCUDAKNNSELF_COMPACT).
+//   lists [n*k] sorted-space neighbours, pos [3n] SoA sorted normalised,
+//   perm [n], ext [2], level [n] (optional): level at which the query stopped
+//   (0..7, 8 = ran out of levels), kth [n] (optional): k-th distance (1e10 if < k).
+// Returns the number of invalid queries.
+int orc_knn(const float* xyz, int n, int k, int* lists, float* pos, int* perm, float* ext,
+            int* level, float* kth, long long* visited_total) {
+    Grid g;
+    build_grid(xyz, n, g, kLevels);
+    float thres = 1e8f;
+    thres /= (g.mx - g.mn);
+    thres *= thres;
+    int invalid_count = 0;
+    long long visited_sum = 0;
+#pragma omp parallel reduction(+ : invalid_count, visited_sum)
+    {
+        std::vector<float> dist(k);
+#pragma omp for schedule(dynamic, 256)
+        for (int q = 0; q < n; q++) {
+            int counter;
+            bool invalid;
+            long long visited = 0;
+            int lv = knn_query(g, q, k, thres, dist.data(), lists + (size_t)q * k, counter, invalid, visited);
+            visited_sum += visited;
+            if (invalid) invalid_count++;
+            if (level) level[q] = lv;
+            if (kth) kth[q] = counter == k ? dist[k - 1] : 1e10f;
+        }
+    }
+    for (int s = 0; s < n; s++) {
+        pos[s] = g.x[s]; pos[n + s] = g.y[s]; pos[2 * (size_t)n + s] = g.z[s];
+        perm[s] = g.perm[s];
+    }
+    ext[0] = g.mn; ext[1] = g.mx;
+    if (visited_total) *visited_total = visited_sum;
+    return invalid_count;
+}
+
+// Mesh 1-ring lists of GridMeshCuda (GridMeshCuda1.cu:314-511).  Each vertex
+// receives the other two corners of every triangle it belongs to, inserted with
+// the same admission rule as the grid kNN (strict '<' at slot k, dedup,
+// FindPosition).  The reference visits a vertex's triangles in a racy order
+// (one atomicExch winner per pass, GridMeshCuda1.cu:110-116); here they are
+// visited in ascending triangle order, which fixes the order of equal distances.
+// Triangles with any index >= n are skipped (the reference remaps them through
+// an out-of-range read, GridMeshCuda1.cu:224-232).
+void orc_mesh_1ring(const float* xyz, int n, const uint32_t* tris, int t, int k, int* lists, float* pos,
+                    int* perm, float* ext) {
+    Grid g;
+    build_grid(xyz, n, g, 1);
+    std::vector<int> rev(n);
+    for (int s = 0; s < n; s++) rev[g.perm[s]] = s;
+    // corners grouped by vertex in ascending triangle order
+    std::vector<int> cnt(n + 1, 0);
+    for (int i = 0; i < t; i++) {
+        uint32_t v0 = tris[3 * (size_t)i], v1 = tris[3 * (size_t)i + 1], v2 = tris[3 * (size_t)i + 2];
+        if (v0 >= (uint32_t)n || v1 >= (uint32_t)n || v2 >= (uint32_t)n) continue;
+        for (int c = 0; c < 3; c++) cnt[rev[tris[3 * (size_t)i + c]] + 1]++;
+    }
+    for (int v = 0; v < n; v++) cnt[v + 1] += cnt[v];
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1), corner((size_t)cnt[n]);
+    for (int i = 0; i < t; i++) {
+        uint32_t v0 = tris[3 * (size_t)i], v1 = tris[3 * (size_t)i + 1], v2 = tris[3 * (size_t)i + 2];
+        if (v0 >= (uint32_t)n || v1 >= (uint32_t)n || v2 >= (uint32_t)n) continue;
+        for (int c = 0; c < 3; c++) corner[fill[rev[tris[3 * (size_t)i + c]]]++] = 3 * i + c;
+    }
+#pragma omp parallel
+    {
+        std::vector<float> dist(k);
+#pragma omp for schedule(dynamic, 1024)
+        for (int v = 0; v < n; v++) {
+            int* idx = lists + (size_t)v * k;
+            for (int i = 0; i < k; i++) { dist[i] = 1e10f; idx[i] = -1; }
+            int counter = 0;
+            for (int e = cnt[v]; e < cnt[v + 1]; e++) {
+                int tri = corner[e] / 3, c1 = corner[e] % 3;
+                for (int c2 = 0; c2 < 3; c2++) {
+                    if (c2 == c1) continue;
+                    int u = rev[tris[3 * (size_t)tri + c2]];
+                    float d = dist3(g.x[v], g.y[v], g.z[v], g.x[u], g.y[u], g.z[u]);
+                    append(dist.data(), idx, k, counter, d, u);
+                }
+            }
+        }
+    }
+    for (int s = 0; s < n; s++) {
+        pos[s] = g.x[s]; pos[n + s] = g.y[s]; pos[2 * (size_t)n + s] = g.z[s];
+        perm[s] = g.perm[s];
+    }
+    ext[0] = g.mn; ext[1] = g.mx;
+}
+
+// EGT filter (calculateEGG_GKNN, EGT_CUDA.cu:172-189): out = lists with the
+// rejected entries set to -1.  in and out may alias.
+void orc_egt(const float* pos, int n, int k, const int* lists_in, float alpha, int* lists_out) {
+    const float* X = pos;
+    const float* Y = pos + n;
+    const float* Z = pos + 2 * (size_t)n;
+#pragma omp parallel
+    {
+        std::vector<int> row(k);
+#pragma omp for schedule(dynamic, 256)
+        for (int i = 0; i < n; i++) {
+            std::memcpy(row.data(), lists_in + (size_t)i * k, sizeof(int) * k);
+            int* out = lists_out + (size_t)i * k;
+            for (int j = 0; j < k; j++) out[j] = row[j];
+            for (int j = k - 1; j >= 0; j--)
+                if (row[j] != -1 && !egt_keep(X, Y, Z, row.data(), j, X[i], Y[i], Z[i], alpha)) out[j] = -1;
+        }
+    }
+}
+
+// Taubin lambda/mu smoothing (taubin_step_GKNN EGT_CUDA.cu:229-276, loop
+// EGT_CUDA.cu:559-633) in float, weights exp(-d^2), isRegularized = 0.
+void orc_taubin_f32(float* pos, int n, int k, const int* lists, int iters, float lambda, float mu) {
+    std::vector<float> tmp(3 * (size_t)n);
+    float* in = pos;
+    float* out = tmp.data();
+    for (int it = 0; it < 2 * iters; it++) {
+        const float scale = (it & 1) ? mu : lambda;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; i++) {
+            float x1 = in[i], y1 = in[n + i], z1 = in[2 * (size_t)n + i];
+            float cx = 0, cy = 0, cz = 0, sum = 0;
+            const int* row = lists + (size_t)i * k;
+            for (int j = 0; j < k; j++) {
+                int m = row[j];
+                if (m == -1) continue;
+                float x2 = in[m], y2 = in[n + m], z2 = in[2 * (size_t)n + m];
+                float w = std::exp(-dist3(x1, y1, z1, x2, y2, z2));
+                cx = acc(cx, w, x2 - x1); cy = acc(cy, w, y2 - y1); cz = acc(cz, w, z2 - z1);
+                sum += w;
+            }
+            if (sum == 0.0f) sum = 1e-8f;
+            out[i] = x1 + scale * cx / sum;
+            out[n + i] = y1 + scale * cy / sum;
+            out[2 * (size_t)n + i] = z1 + scale * cz / sum;
+        }
+        std::swap(in, out);
+    }
+    if (in != pos) std::memcpy(pos, in, sizeof(float) * 3 * (size_t)n);
+}
+
+// Same iteration in double precision (the FP64 oracle).
+void orc_taubin_f64(double* pos, int n, int k, const int* lists, int iters, double lambda, double mu) {
+    std::vector<double> tmp(3 * (size_t)n);
+    double* in = pos;
+    double* out = tmp.data();
+    for (int it = 0; it < 2 * iters; it++) {
+        const double scale = (it & 1) ? mu : lambda;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; i++) {
+            double x1 = in[i], y1 = in[n + i], z1 = in[2 * (size_t)n + i];
+            double cx = 0, cy = 0, cz = 0, sum = 0;
+            const int* row = lists + (size_t)i * k;
+            for (int j = 0; j < k; j++) {
+                int m = row[j];
+                if (m == -1) continue;
+                double dx = in[m] - x1, dy = in[n + m] - y1, dz = in[2 * (size_t)n + m] - z1;
+                double w = std::exp(-(dx * dx + dy * dy + dz * dz));
+                cx += w * dx; cy += w * dy; cz += w * dz;
+                sum += w;
+            }
+            if (sum == 0.0) sum = 1e-8;
+            out[i] = x1 + scale * cx / sum;
+            out[n + i] = y1 + scale * cy / sum;
+            out[2 * (size_t)n + i] = z1 + scale * cz / sum;
+        }
+        std::swap(in, out);
+    }
+    if (in != pos) std::memcpy(pos, in, sizeof(double) * 3 * (size_t)n);
+}
+
+// Unoriented PCA normals (calculateNormal Normal_CUDA.cu:87-144) in sorted
+// space: out [3n] SoA.  use_f64 selects the FP64 oracle.
+void orc_normals(const float* pos, int n, int k, const int* lists, int use_f64, float* out) {
+    const float* X = pos;
+    const float* Y = pos + n;
+    const float* Z = pos + 2 * (size_t)n;
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int i = 0; i < n; i++) {
+        if (use_f64) {
+            double v[3];
+            normal_of<double>(X, Y, Z, lists + (size_t)i * k, k, i, v);
+            out[i] = (float)v[0]; out[n + i] = (float)v[1]; out[2 * (size_t)n + i] = (float)v[2];
+        } else {
+            float v[3];
+            normal_of<float>(X, Y, Z, lists + (size_t)i * k, k, i, v);
+            out[i] = v[0]; out[n + i] = v[1]; out[2 * (size_t)n + i] = v[2];
+        }
+    }
+}
+
+// Orientation of GetNormals (Normal_CUDA.cu:329-711) on sorted-space normals,
+// in place.  Undirected edges (min,max) from the lists with weight
+// max(0, 1-|n_u.n_v|) (Normal_CUDA.cu:146-175), deduplicated by the key
+// u*n+v and ordered by (weight, key) (Normal_CUDA.cu:363-385).  The spanning
+// forest is the minimum one for that total order (Kruskal); the reference's
+// Borůvka (CUDA_MST.cu:296-418) computes a minimum forest with its own tie
+// rule.  Each tree is traversed breadth-first from the first vertex `u` of its
+// lightest edge (for the first tree this is the reference's root,
+// Normal_CUDA.cu:438-440), flipping a child whose normal has a negative dot
+// product with its parent's (bfs.cu:21-29).  Component sign votes
+// (Normal_CUDA.cu:517-711) are applied over list edges that join trees.
+// Outputs (optional): parent [n] (-1 roots/untouched), ncomp.
+int orc_orient(int n, int k, const int* lists, float* nrm, int* parent) {
+    float* NX = nrm;
+    float* NY = nrm + n;
+    float* NZ = nrm + 2 * (size_t)n;
+    struct E { float w; long long key; int u, v; };
+    std::vector<E> edges;
+    edges.reserve((size_t)n * 8);
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < k; j++) {
+            int m = lists[(size_t)i * k + j];
+            if (m < 0) continue;
+            int u = std::min(i, m), v = std::max(i, m);
+            float dp = dot3(NX[i], NY[i], NZ[i], NX[m], NY[m], NZ[m]);
+            float w = std::fmax(0.0f, 1.0f - std::fabs(dp));
+            edges.push_back({w, (long long)u * n + v, u, v});
+        }
+    std::sort(edges.begin(), edges.end(), [](const E& a, const E& b) { return a.key < b.key; });
+    edges.erase(std::unique(edges.begin(), edges.end(), [](const E& a, const E& b) { return a.key == b.key; }),
+                edges.end());
+    std::stable_sort(edges.begin(), edges.end(), [](const E& a, const E& b) { return a.w < b.w; });
+    DSU dsu(n);
+    std::vector<std::vector<int>> adj(n);
+    for (const E& e : edges) {
+        if (e.u == e.v) continue;
+        if (dsu.unite(e.u, e.v)) { adj[e.u].push_back(e.v); adj[e.v].push_back(e.u); }
+    }
+    std::vector<int> comp(n, -1), par(n, -1);
+    int ncomp = 0;
+    for (const E& e : edges) {
+        int root = e.u;
+        if (comp[root] >= 0 || adj[root].empty()) continue;
+        std::queue<int> qu;
+        qu.push(root);
+        comp[root] = ncomp;
+        while (!qu.empty()) {
+            int a = qu.front(); qu.pop();
+            for (int b : adj[a]) {
+                if (comp[b] >= 0) continue;
+                comp[b] = ncomp;
+                par[b] = a;
+                float dp = dot3(NX[a], NY[a], NZ[a], NX[b], NY[b], NZ[b]);
+                if (dp < 0) { NX[b] = -NX[b]; NY[b] = -NY[b]; NZ[b] = -NZ[b]; }
+                qu.push(b);
+            }
+        }
+        ncomp++;
+    }
+    // component votes (componentCounter Normal_CUDA.cu:271-290) and the
+    // component-graph BFS (Normal_CUDA.cu:657-711)
+    if (ncomp > 1) {
+        std::vector<std::vector<int>> votes(ncomp);
+        std::vector<std::set<std::pair<int, int>>> cg(ncomp);
+        for (int c = 0; c < ncomp; c++) {
+            std::vector<int> cnt(ncomp, 0);
+            for (int i = 0; i < n; i++) {
+                if (comp[i] != c) continue;
+                for (int j = 0; j < k; j++) {
+                    int m = lists[(size_t)i * k + j];
+                    if (m < 0 || comp[m] < 0 || comp[m] == c) continue;
+                    float dp = dot3(NX[i], NY[i], NZ[i], NX[m], NY[m], NZ[m]);
+                    cnt[comp[m]] += dp > 0 ? 1 : -1;
+                }
+            }
+            for (int o = 0; o < ncomp; o++) {
+                if (cnt[o] == 0) continue;
+                int orient = cnt[o] > 0 ? 1 : -1;
+                cg[c].insert({o, orient});
+                cg[o].insert({c, orient});
+            }
+        }
+        std::vector<char> seen(ncomp, 0);
+        std::vector<int> flip(ncomp, 0);
+        for (int r = 0; r < ncomp; r++) {
+            if (seen[r]) continue;
+            std::queue<std::pair<int, int>> qq;
+            qq.push({r, 1});
+            seen[r] = 1;
+            while (!qq.empty()) {
+                auto [c, o] = qq.front(); qq.pop();
+                for (auto [nb, ori] : cg[c]) {
+                    if (seen[nb]) continue;
+                    if (o * ori < 0) flip[nb] = 1;
+                    qq.push({nb, o * ori});
+                    seen[nb] = 1;
+                }
+            }
+        }
+        for (int i = 0; i < n; i++)
+            if (comp[i] >= 0 && flip[comp[i]]) { NX[i] = -NX[i]; NY[i] = -NY[i]; NZ[i] = -NZ[i]; }
+    }
+    if (parent) std::memcpy(parent, par.data(), sizeof(int) * n);
+    return ncomp;
+}
+
+// getOutputPoints (getOutputPoints.cu:9-63): denormalise and scatter to the
+// original order.  pos [3n] sorted SoA -> out [3n] original-order SoA.
+void orc_output(const float* pos, const int* perm, const float* ext, int n, float* out) {
+    const float d = ext[1] - ext[0];
+    for (int s = 0; s < n; s++) {
+        int o = perm[s];
+        out[o] = denorm(pos[s], d, ext[0]);
+        out[n + o] = denorm(pos[n + s], d, ext[0]);
+        out[2 * (size_t)n + o] = denorm(pos[2 * (size_t)n + s], d, ext[0]);
+    }
+}
+
+// Exact brute-force kNN over sorted-space positions, ordered by (distance,
+// index), used to check that the grid search is exact.  dist [n*k].
+void orc_bruteforce(const float* pos, int n, int k, int* lists, float* dists) {
+    const float* X = pos;
+    const float* Y = pos + n;
+    const float* Z = pos + 2 * (size_t)n;
+#pragma omp parallel
+    {
+        std::vector<std::pair<float, int>> c((size_t)n);
+#pragma omp for schedule(dynamic, 64)
+        for (int q = 0; q < n; q++) {
+            int m = 0;
+            for (int p = 0; p < n; p++)
+                if (p != q) c[m++] = {dist3(X[q], Y[q], Z[q], X[p], Y[p], Z[p]), p};
+            int kk = std::min(k, m);
+            std::partial_sort(c.begin(), c.begin() + kk, c.begin() + m);
+            for (int j = 0; j < k; j++) {
+                lists[(size_t)q * k + j] = j < kk ? c[j].second : -1;
+                dists[(size_t)q * k + j] = j < kk ? c[j].first : 1e10f;
+            }
+        }
+    }
+}
+
+}  // extern "C"

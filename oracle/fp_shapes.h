@@ -1,0 +1,55 @@
+// Rounding shapes of the reference's floating-point expressions.
+//
+// ORACLE / TEST INFRASTRUCTURE.  The reference is compiled by nvcc with the
+// default --fmad=true, so a*b+c style expressions are contracted into fused
+// multiply-adds.  Which operand pair is fused decides the last bit of the
+// result, and the last bit decides ties and near-ties in the kNN ordering.
+// The shapes below were identified black-box (a probe kernel compiled with the
+// same flags, evaluated on random inputs and compared against each candidate
+// written with an explicit fma); the CUDA kernels use the same shapes through
+// __fmaf_rn/__fmul_rn/__fadd_rn so that they, this oracle and the reference
+// round identically.  The CPU side must be compiled with -ffp-contract=off.
+#pragma once
+#include <cmath>
+
+namespace fpshape {
+
+// (ax-bx)^2 + (ay-by)^2 + (az-bz)^2  (GridKNNCuda.cu:91-99, EGT_CUDA.cu:34-37)
+inline float dist3(float ax, float ay, float az, float bx, float by, float bz) {
+    float dx = ax - bx, dy = ay - by, dz = az - bz;
+    return std::fmaf(dz, dz, std::fmaf(dx, dx, dy * dy));
+}
+// x*x + y*y + z*z  (EGT_CUDA.cu:53-56, 147)
+inline float sq3(float x, float y, float z) { return std::fmaf(z, z, std::fmaf(x, x, y * y)); }
+// a.b  (Normal_CUDA.cu:168, bfs.cu:22-23)
+inline float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+    return std::fmaf(az, bz, std::fmaf(ax, bx, ay * by));
+}
+// x - xmin - f*h   (GridKNNCuda.cu:717-739 lower faces)
+inline float face_lo(float x, float xmin, float f, float h) { return std::fmaf(-f, h, x - xmin); }
+// xmin - x + f*h   (GridKNNCuda.cu:717-739 upper faces)
+inline float face_hi(float x, float xmin, float f, float h) { return std::fmaf(f, h, xmin - x); }
+// u2*v3 - v2*u3  (EGT_CUDA.cu:97-104)
+inline float cross1(float u2, float v3, float v2, float u3) { return std::fmaf(u2, v3, -(v2 * u3)); }
+// a11*x + a12*y + a13*z + a14  (EGT_CUDA.cu:106-115)
+inline float affine(float a1, float a2, float a3, float a4, float x, float y, float z) {
+    return std::fmaf(a3, z, std::fmaf(a1, x, a2 * y)) + a4;
+}
+// x*x + y*y/aa + z*z/aa  (EGT_CUDA.cu:165)
+inline float ellipsoid(float x, float y, float z, float aa) {
+    return std::fmaf(x, x, (y * y) / aa) + (z * z) / aa;
+}
+// c += w*(q-p)  (EGT_CUDA.cu:266-268)
+inline float acc(float c, float w, float d) { return std::fmaf(w, d, c); }
+// x*d + min  (getOutputPoints.cu:15-17)
+inline float denorm(float x, float d, float mn) { return std::fmaf(x, d, mn); }
+// c*a + s*b  (EigenSolver.cuh:150-156 and the Givens/Householder updates)
+inline float lin2_add(float c, float a, float s, float b) { return std::fmaf(c, a, s * b); }
+// s*a - c*b
+inline float lin2_sub(float s, float a, float c, float b) { return std::fmaf(s, a, -(c * b)); }
+// u*u + v*v  (EigenSolver.cuh:357)
+inline float sq2(float u, float v) { return std::fmaf(u, u, v * v); }
+// c += x*y  (Normal_CUDA.cu:113-121)
+inline float cov_acc(float c, float x, float y) { return std::fmaf(x, y, c); }
+
+}  // namespace fpshape
