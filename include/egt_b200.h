@@ -1,0 +1,147 @@
+/*
+ * egt_b200.h -- C ABI of the B200-native grid kNN / elliptic-Gabriel / Taubin /
+ * normals path.  Plain pointers and sizes only; every call returns an
+ * egt_status (0 = success, negative = error) and takes an explicit CUDA stream
+ * (cudaStream_t passed as void*, NULL = legacy default stream).
+ *
+ * The reference (agalex1974/MultiGPUEGTSmoothing) has no C ABI; its drop-in
+ * boundary is the C++ provider class KNNInterface (KNNInterface.cuh:8-31) and
+ * the classes that produce and consume it.  Each entry point below names the
+ * reference interface it replaces.  A handle owns every device buffer, like the
+ * reference providers do (GridKNNCuda.cu:1005-1021).  Handles are not
+ * thread-safe; separate handles on separate streams are independent.
+ *
+ * Index spaces: "sorted" = cell-sorted order produced at creation (the order
+ * of the reference's device arrays, GridKNNCuda.cu:1114-1128); "original" =
+ * input order.  Device positions are normalised into the unit cube with one
+ * scalar extent for all axes (GridKNNCuda.cu:1042-1071).
+ */
+#ifndef EGT_B200_H
+#define EGT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int egt_status;
+#define EGT_OK                 0
+#define EGT_ERR_CUDA          -1  /* a CUDA runtime call failed (see egt_last_error) */
+#define EGT_ERR_ARG           -2  /* invalid argument (null pointer, n/k out of range) */
+#define EGT_ERR_CAP_EXCEEDED  -3  /* a bounded loop or buffer cap was exceeded */
+#define EGT_ERR_TIMEOUT       -4  /* a bounded device wait expired */
+#define EGT_ERR_STATE         -5  /* call out of order (e.g. smoothing before kNN) */
+#define EGT_ERR_NOMEM         -6  /* device allocation failed */
+
+typedef struct egt_handle egt_handle;
+
+/* Tunables.  Defaults reproduce the reference CLI (main.cpp:108-116). */
+typedef struct egt_config {
+    int device;              /* CUDA device ordinal (default 0) */
+    float eps;               /* cube widening, GridStructure eps (1e-6) */
+    int bucket_count;        /* level-0 buckets per axis (1024) */
+    float threshold;         /* GRIDCUDAKNNSELF_COMPACT thres before scaling (1e8) */
+    int max_points_in_cell;  /* MAX_PNTS_IN_CUBE (100000): larger cells invalidate a query */
+    int knn_mode;            /* 0 = plain hierarchical ring search, 1 = learned proposal */
+    int warps_per_block;     /* kNN/EGT launch shape (0 = autotuned default) */
+    float normals_gap_tol;   /* FP64 eigensolve when (l1-l0) < tol*l2 (0.1; 0 = FP32 only) */
+} egt_config;
+
+/* Device views for the KNNInterface adapter (include/egt_knn_interface.hpp). */
+typedef struct egt_views {
+    float* x;                /* [n] sorted, normalised (GetRefPointsX()[0]) */
+    float* y;                /* [n] (GetRefPointsY()[0]) */
+    float* z;                /* [n] (GetRefPointsZ()[0]) */
+    int* lists;              /* [n*k] sorted-space lists, -1 padded (GetKNNIndexesInPartitions()[0]) */
+    int* perm;               /* [n] sorted slot -> original index (GetOriginalRefIndexes()[0]) */
+    float* normals;          /* [3n] SoA sorted-space normals after egt_normals, else NULL */
+    int64_t n;               /* pointsRefCount() */
+    int k;                   /* NeighborCount() (0 before a neighbour search) */
+    float min_extent;        /* GetMinExtent() */
+    float max_extent;        /* GetMaxExtent() */
+} egt_views;
+
+/* Per-stage device times of the last calls on a handle, in milliseconds. */
+typedef struct egt_timings {
+    float grid_ms, knn_ms, egt_ms, taubin_ms, normals_ms, orient_ms, output_ms;
+    int levels_used;         /* deepest hierarchy level any query reached (0..7) */
+    int64_t invalid_queries; /* rows set to -1 by the invalidation rules */
+    int64_t csr_nnz;         /* neighbours kept by the EGT filter */
+    int64_t normals_fp64;    /* points whose normal was re-solved in FP64 */
+    int64_t msf_edges;       /* edges of the orientation spanning forest */
+    int components;          /* orientation components (trees with >= 1 edge) */
+} egt_timings;
+
+void egt_default_config(egt_config* cfg);
+const char* egt_last_error(void);
+const char* egt_version(void);
+
+/* GridStructure(mesh, 1, eps, 1024, 4) (GridKNNCuda.cu:1165-1205 + InitStructure
+ * :1023-1133): copies n points (AoS xyz, host memory), normalises them, sorts
+ * them by cell and builds the cell hierarchy. */
+egt_status egt_create_cloud(const float* xyz_host, int64_t n, const egt_config* cfg, void* stream,
+                            egt_handle** out);
+/* Same, with the points already in device memory (AoS xyz). */
+egt_status egt_create_cloud_device(const float* xyz_dev, int64_t n, const egt_config* cfg, void* stream,
+                                   egt_handle** out);
+/* GridMeshCuda(mesh, 1, eps, 1024) (GridMeshCuda1.cu:247-414): points plus
+ * t triangles (uint32 vertex indices, host memory). */
+egt_status egt_create_mesh(const float* xyz_host, int64_t n, const uint32_t* tris_host, int64_t t,
+                           const egt_config* cfg, void* stream, egt_handle** out);
+
+/* Re-runs InitStructure for new positions of the same n points (device AoS
+ * xyz), reusing every buffer of the handle: normalisation, cell sort and
+ * hierarchy are rebuilt, previous lists/CSR/normals are invalidated. */
+egt_status egt_update_points_device(egt_handle* h, const float* xyz_dev, void* stream);
+
+/* GridStructure::GRIDCUDAKNNSELF_COMPACT(k, thres) (GridKNNCuda.cu:2322-2634). */
+egt_status egt_knn(egt_handle* h, int k, void* stream);
+/* GridMeshCuda::GetNeighborsFromTriangles(k) (GridMeshCuda1.cu:416-511). */
+egt_status egt_mesh_1ring(egt_handle* h, int k, void* stream);
+
+/* EGT_CUDA::PerformSmoothing(iters, lambda, mu, alpha) (EGT_CUDA.cu:476-648):
+ * the elliptic-Gabriel filter followed by iters lambda/mu Taubin iterations. */
+egt_status egt_smooth(egt_handle* h, int iters, float lambda, float mu, float alpha, void* stream);
+/* The two halves of egt_smooth: calculateEGG_GKNN (EGT_CUDA.cu:172-189, :505-530)
+ * and the Taubin loop (EGT_CUDA.cu:229-276, :559-633). */
+egt_status egt_filter(egt_handle* h, float alpha, void* stream);
+egt_status egt_taubin(egt_handle* h, int iters, float lambda, float mu, void* stream);
+
+/* Normal_CUDA::GetNormals(nx, ny, nz) (Normal_CUDA.cu:304-775): oriented
+ * normals in original order, written to host (or NULL to keep them on device). */
+egt_status egt_normals(egt_handle* h, float* nx, float* ny, float* nz, void* stream);
+
+/* getOutputPoints(x, y, z, provider) (getOutputPoints.cu:34-63): denormalised
+ * positions in original order, written to host memory. */
+egt_status egt_output(egt_handle* h, float* x, float* y, float* z, void* stream);
+/* Same, written to device memory (SoA, original order). */
+egt_status egt_output_device(egt_handle* h, float* x, float* y, float* z, void* stream);
+
+/* KNNInterface::GetKNNIndexes (GridKNNCuda.cu:1941-1968): n*k host ints in
+ * original ids and original row order. */
+egt_status egt_get_knn_host(egt_handle* h, int* knn_host, void* stream);
+/* Device pointers behind the KNNInterface getters. */
+egt_status egt_get_views(egt_handle* h, egt_views* views);
+/* Per-stage device timings of the last calls (filled when the stream is synced). */
+egt_status egt_get_timings(egt_handle* h, egt_timings* t);
+/* Sorted-space EGT-filtered neighbourhoods as CSR (device pointers, valid
+ * until the next call on the handle): offsets [n+1], cols [nnz]. */
+egt_status egt_get_csr(egt_handle* h, const int** offsets, const int** cols, int64_t* nnz);
+
+/* Copies bytes from device memory (e.g. a pointer from egt_get_views) to host
+ * memory after synchronising the handle's stream.  No reference counterpart:
+ * lets hosts without their own CUDA runtime binding read the device views. */
+egt_status egt_copy_to_host(egt_handle* h, void* dst_host, const void* src_dev, int64_t bytes);
+
+/* Number of kernels this library has launched from the calling host thread
+ * (all handles).  No reference counterpart: benchmark accounting. */
+int64_t egt_kernel_launches(void);
+
+/* ~GridStructure / ~GridMeshCuda: frees every device buffer of the handle. */
+void egt_destroy(egt_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EGT_B200_H */

@@ -1,0 +1,344 @@
+// C ABI of libegt_b200 (declared in include/egt_b200.h): handle lifecycle,
+// argument checking, error reporting and the stage entry points.
+#include <cstring>
+#include <mutex>
+#include <string>
+#include "egt_internal.cuh"
+
+namespace egt {
+
+static thread_local std::string g_error;
+static thread_local int64_t g_launches = 0;
+
+void count_launch() { g_launches++; }
+
+void set_error(const std::string& msg) { g_error = msg; }
+
+std::string cuda_msg(cudaError_t e, const char* what, const char* file, int line) {
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "%s failed: %s (%s) at %s:%d", what, cudaGetErrorName(e),
+                  cudaGetErrorString(e), file, line);
+    return std::string(buf);
+}
+
+float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();
+        return -1.f;
+    }
+    return ms;
+}
+
+}  // namespace egt
+
+using namespace egt;
+
+namespace {
+
+egt_status check_handle(egt_handle* h) {
+    if (!h) { set_error("null handle"); return EGT_ERR_ARG; }
+    return EGT_OK;
+}
+
+void bind_stream(egt_handle* h, void* stream) { h->stream = (cudaStream_t)stream; }
+
+void free_handle(egt_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->cfg.device);
+    auto F = [](void* p) { if (p) cudaFree(p); };
+    F(h->p4); F(h->p4b); F(h->x); F(h->y); F(h->z); F(h->cell0); F(h->perm); F(h->d_norm);
+    for (int L = 0; L < kMaxLevels; L++) {
+        F(h->lv[L].order); F(h->lv[L].cell_start); F(h->lv[L].cell_x); F(h->lv[L].row_range);
+    }
+    F(h->lists); F(h->kth); F(h->qlevel); F(h->csr_off); F(h->csr_col); F(h->tris); F(h->nrm);
+    F(h->d_counters); F(h->scratch.ptr);
+    if (h->taubin_exec) cudaGraphExecDestroy(h->taubin_exec);
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    delete h;
+}
+
+egt_status create_common(const float* xyz, bool xyz_on_device, int64_t n, const uint32_t* tris, int64_t t,
+                         const egt_config* cfg_in, void* stream, egt_handle** out) {
+    if (!out) { set_error("null output handle pointer"); return EGT_ERR_ARG; }
+    *out = nullptr;
+    if (!xyz) { set_error("null point array"); return EGT_ERR_ARG; }
+    if (n < 1 || n > (int64_t)(1u << 30)) { set_error("point count must be in [1, 2^30]"); return EGT_ERR_ARG; }
+    if (t < 0 || (t > 0 && !tris)) { set_error("invalid triangle array"); return EGT_ERR_ARG; }
+    egt_config cfg;
+    egt_default_config(&cfg);
+    if (cfg_in) cfg = *cfg_in;
+    if (cfg.bucket_count != 1024) {
+        set_error("bucket_count must be 1024 (the reference's level-0 grid)");
+        return EGT_ERR_ARG;
+    }
+    if (cfg.max_points_in_cell < 1) { set_error("max_points_in_cell must be >= 1"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(cfg.device));
+    egt_handle* h = new egt_handle();
+    h->cfg = cfg;
+    h->n = n;
+    h->is_mesh = tris != nullptr;
+    h->t = t;
+    bind_stream(h, stream);
+    auto fail = [&](egt_status s) { free_handle(h); return s; };
+#define CREATE_TRY(call)                                                     \
+    do {                                                                     \
+        cudaError_t e__ = (call);                                            \
+        if (e__ != cudaSuccess) {                                            \
+            set_error(cuda_msg(e__, #call, __FILE__, __LINE__));             \
+            return fail(e__ == cudaErrorMemoryAllocation ? EGT_ERR_NOMEM : EGT_ERR_CUDA); \
+        }                                                                    \
+    } while (0)
+    CREATE_TRY(cudaMalloc(&h->p4, sizeof(float4) * n));
+    CREATE_TRY(cudaMalloc(&h->x, sizeof(float) * n));
+    CREATE_TRY(cudaMalloc(&h->y, sizeof(float) * n));
+    CREATE_TRY(cudaMalloc(&h->z, sizeof(float) * n));
+    CREATE_TRY(cudaMalloc(&h->cell0, sizeof(uint32_t) * n));
+    CREATE_TRY(cudaMalloc(&h->perm, sizeof(int) * n));
+    CREATE_TRY(cudaMalloc(&h->d_norm, sizeof(NormParams)));
+    CREATE_TRY(cudaMalloc(&h->d_counters, sizeof(unsigned long long) * kCtrWords));
+    CREATE_TRY(cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * kCtrWords, h->stream));
+    for (auto& e : h->ev) CREATE_TRY(cudaEventCreate(&e));
+    const float* dxyz = xyz;
+    float* staged = nullptr;
+    if (!xyz_on_device) {
+        CREATE_TRY(cudaMallocAsync((void**)&staged, sizeof(float) * 3 * n, h->stream));
+        CREATE_TRY(cudaMemcpyAsync(staged, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, h->stream));
+        dxyz = staged;
+    }
+    if (tris && t > 0) {
+        CREATE_TRY(cudaMalloc(&h->tris, sizeof(uint32_t) * 3 * t));
+        CREATE_TRY(cudaMemcpyAsync(h->tris, tris, sizeof(uint32_t) * 3 * t, cudaMemcpyHostToDevice, h->stream));
+    }
+    egt_status s = build_grid(h, dxyz, h->is_mesh ? 1 : kMaxLevels);
+    if (staged) cudaFreeAsync(staged, h->stream);
+    if (s != EGT_OK) return fail(s);
+    CREATE_TRY(cudaStreamSynchronize(h->stream));
+#undef CREATE_TRY
+    h->tm.grid_ms = elapsed_ms(h->ev[0], h->ev[1]);
+    *out = h;
+    return EGT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void egt_default_config(egt_config* cfg) {
+    if (!cfg) return;
+    cfg->device = 0;
+    cfg->eps = 1e-6f;
+    cfg->bucket_count = 1024;
+    cfg->threshold = 1e8f;
+    cfg->max_points_in_cell = 100000;
+    cfg->knn_mode = 0;
+    cfg->warps_per_block = 0;
+    cfg->normals_gap_tol = 0.1f;
+}
+
+const char* egt_last_error(void) { return g_error.c_str(); }
+
+const char* egt_version(void) { return "egt_b200 1.0 (sm_100a)"; }
+
+egt_status egt_create_cloud(const float* xyz_host, int64_t n, const egt_config* cfg, void* stream,
+                            egt_handle** out) {
+    return create_common(xyz_host, false, n, nullptr, 0, cfg, stream, out);
+}
+
+egt_status egt_create_cloud_device(const float* xyz_dev, int64_t n, const egt_config* cfg, void* stream,
+                                   egt_handle** out) {
+    return create_common(xyz_dev, true, n, nullptr, 0, cfg, stream, out);
+}
+
+egt_status egt_create_mesh(const float* xyz_host, int64_t n, const uint32_t* tris_host, int64_t t,
+                           const egt_config* cfg, void* stream, egt_handle** out) {
+    if (!tris_host || t < 1) { set_error("a mesh needs at least one triangle"); return EGT_ERR_ARG; }
+    return create_common(xyz_host, false, n, tris_host, t, cfg, stream, out);
+}
+
+egt_status egt_update_points_device(egt_handle* h, const float* xyz_dev, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (!xyz_dev) { set_error("egt_update_points_device: null points"); return EGT_ERR_ARG; }
+    if (h->is_mesh) { set_error("egt_update_points_device: point-cloud handles only"); return EGT_ERR_STATE; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    h->have_csr = false;
+    if (h->nrm) { cudaFree(h->nrm); h->nrm = nullptr; }
+    return build_grid(h, xyz_dev, kMaxLevels);
+}
+
+int64_t egt_kernel_launches(void) { return g_launches; }
+
+egt_status egt_knn(egt_handle* h, int k, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (h->is_mesh) { set_error("egt_knn: mesh handles take their neighbours from triangles"); return EGT_ERR_STATE; }
+    if ((int64_t)k * h->n > (int64_t)0x7fffffff) { set_error("egt_knn: n*k exceeds 2^31-1"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    return run_knn(h, k);
+}
+
+egt_status egt_mesh_1ring(egt_handle* h, int k, void* stream) {
+    EGT_TRY(check_handle(h));
+    if ((int64_t)k * h->n > (int64_t)0x7fffffff) { set_error("egt_mesh_1ring: n*k exceeds 2^31-1"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    return run_mesh_1ring(h, k);
+}
+
+egt_status egt_filter(egt_handle* h, float alpha, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (!(alpha > 0.f)) { set_error("egt_filter: alpha must be > 0"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    return run_egt(h, alpha);
+}
+
+egt_status egt_taubin(egt_handle* h, int iters, float lambda, float mu, void* stream) {
+    EGT_TRY(check_handle(h));
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    return run_taubin(h, iters, lambda, mu);
+}
+
+egt_status egt_smooth(egt_handle* h, int iters, float lambda, float mu, float alpha, void* stream) {
+    EGT_TRY(egt_filter(h, alpha, stream));
+    return egt_taubin(h, iters, lambda, mu, stream);
+}
+
+egt_status egt_normals(egt_handle* h, float* nx, float* ny, float* nz, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (h->is_mesh) { set_error("egt_normals: normals are computed for point clouds only"); return EGT_ERR_STATE; }
+    if (!h->lists) { set_error("egt_normals: no neighbour lists"); return EGT_ERR_STATE; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    EGT_TRY(run_normals(h));
+    EGT_TRY(run_orient(h));
+    if (nx || ny || nz) {
+        if (!nx || !ny || !nz) { set_error("egt_normals: give all three outputs or none"); return EGT_ERR_ARG; }
+        const int64_t n = h->n;
+        float* tmp = nullptr;
+        EGT_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 3 * n, h->stream));
+        // scatter sorted-space normals to original order (rearrange_output, Normal_CUDA.cu:745-759)
+        EGT_TRY(scatter_original(h, h->nrm, tmp));
+        EGT_CUDA_TRY(cudaMemcpyAsync(nx, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+        EGT_CUDA_TRY(cudaMemcpyAsync(ny, tmp + n, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+        EGT_CUDA_TRY(cudaMemcpyAsync(nz, tmp + 2 * n, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+        cudaFreeAsync(tmp, h->stream);
+        EGT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+    return EGT_OK;
+}
+
+egt_status egt_output_device(egt_handle* h, float* x, float* y, float* z, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (!x || !y || !z) { set_error("egt_output: null output"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    return run_output(h, x, y, z);
+}
+
+egt_status egt_output(egt_handle* h, float* x, float* y, float* z, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (!x || !y || !z) { set_error("egt_output: null output"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    const int64_t n = h->n;
+    float* tmp = nullptr;
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 3 * n, h->stream));
+    egt_status s = run_output(h, tmp, tmp + n, tmp + 2 * n);
+    if (s == EGT_OK) {
+        EGT_CUDA_TRY(cudaMemcpyAsync(x, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+        EGT_CUDA_TRY(cudaMemcpyAsync(y, tmp + n, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+        EGT_CUDA_TRY(cudaMemcpyAsync(z, tmp + 2 * n, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+    }
+    cudaFreeAsync(tmp, h->stream);
+    EGT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return s;
+}
+
+egt_status egt_get_knn_host(egt_handle* h, int* knn_host, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (!knn_host) { set_error("egt_get_knn_host: null output"); return EGT_ERR_ARG; }
+    if (!h->lists) { set_error("egt_get_knn_host: no neighbour lists"); return EGT_ERR_STATE; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    const size_t tot = (size_t)h->n * h->k;
+    int* tmp = nullptr;
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(int) * tot, h->stream));
+    egt_status s = lists_original(h, tmp);
+    if (s == EGT_OK)
+        EGT_CUDA_TRY(cudaMemcpyAsync(knn_host, tmp, sizeof(int) * tot, cudaMemcpyDeviceToHost, h->stream));
+    cudaFreeAsync(tmp, h->stream);
+    EGT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return s;
+}
+
+egt_status egt_get_views(egt_handle* h, egt_views* v) {
+    EGT_TRY(check_handle(h));
+    if (!v) { set_error("egt_get_views: null output"); return EGT_ERR_ARG; }
+    v->x = h->x;
+    v->y = h->y;
+    v->z = h->z;
+    v->lists = h->lists;
+    v->perm = h->perm;
+    v->normals = h->nrm;
+    v->n = h->n;
+    v->k = h->k;
+    v->min_extent = h->norm.mn;
+    v->max_extent = h->norm.mx;
+    return EGT_OK;
+}
+
+egt_status egt_get_csr(egt_handle* h, const int** offsets, const int** cols, int64_t* nnz) {
+    EGT_TRY(check_handle(h));
+    if (!h->lists) { set_error("egt_get_csr: no neighbour lists"); return EGT_ERR_STATE; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    EGT_TRY(ensure_csr(h));
+    if (offsets) *offsets = h->csr_off;
+    if (cols) *cols = h->csr_col;
+    if (nnz) *nnz = h->nnz;
+    return EGT_OK;
+}
+
+egt_status egt_get_timings(egt_handle* h, egt_timings* t) {
+    EGT_TRY(check_handle(h));
+    if (!t) { set_error("egt_get_timings: null output"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    EGT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    unsigned long long ctr[kCtrWords];
+    EGT_CUDA_TRY(cudaMemcpy(ctr, h->d_counters, sizeof(ctr), cudaMemcpyDeviceToHost));
+    h->tm.knn_ms = elapsed_ms(h->ev[2], h->ev[3]);
+    h->tm.egt_ms = elapsed_ms(h->ev[4], h->ev[5]);
+    h->tm.taubin_ms = elapsed_ms(h->ev[6], h->ev[7]);
+    h->tm.normals_ms = elapsed_ms(h->ev[8], h->ev[9]);
+    h->tm.orient_ms = elapsed_ms(h->ev[10], h->ev[11]);
+    h->tm.output_ms = elapsed_ms(h->ev[12], h->ev[13]);
+    h->tm.invalid_queries = (int64_t)ctr[kCtrInvalid];
+    h->tm.levels_used = (int)ctr[kCtrMaxLevel];
+    h->tm.csr_nnz = h->nnz;
+    h->tm.normals_fp64 = (int64_t)ctr[kCtrNormFallback];
+    h->tm.msf_edges = (int64_t)ctr[kCtrMsf];
+    h->tm.components = (int)ctr[kCtrComps];
+    *t = h->tm;
+    return EGT_OK;
+}
+
+egt_status egt_copy_to_host(egt_handle* h, void* dst, const void* src, int64_t bytes) {
+    EGT_TRY(check_handle(h));
+    if (bytes < 0 || (bytes > 0 && (!dst || !src))) { set_error("egt_copy_to_host: bad arguments"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    EGT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (bytes) EGT_CUDA_TRY(cudaMemcpy(dst, src, (size_t)bytes, cudaMemcpyDeviceToHost));
+    return EGT_OK;
+}
+
+void egt_destroy(egt_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->cfg.device);
+    cudaStreamSynchronize(h->stream);
+    free_handle(h);
+}
+
+}  // extern "C"

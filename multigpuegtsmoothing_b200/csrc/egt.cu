@@ -1,0 +1,234 @@
+// Elliptic-Gabriel neighbour filter and CSR compaction.
+//
+// Reference: calculateEGG_GKNN (EGT_CUDA.cu:172-189) with the predicate
+// isEllipicGabrielNeighbor_GKNN (EGT_CUDA.cu:136-170) and its frame helpers
+// (EGT_CUDA.cu:34-134).  Entry j of a query's list is dropped when one of the
+// closer listed neighbours j' < j lies strictly inside the ellipsoid centred on
+// the midpoint of (p, q_j), with half-axis d = |q_j - p|/2 along q_j - p and
+// alpha*d across.  The reference walks j downward and edits the list in place;
+// because only indices >= j have been edited when entry j is tested, every
+// test sees the unfiltered list, which is what this kernel does explicitly.
+//
+// One warp per query: lane l owns list slots l + 32*s.  Each lane builds the
+// local frame of each of its slots once, then the warp broadcasts the closer
+// neighbours one by one (shuffles) and every lane tests them against its
+// slots.  The filtered list is written back in place (-1 for dropped entries,
+// the reference's observable behaviour on GetKNNIndexesInPartitions), the kept
+// count per row feeds a scan, and a second kernel packs the kept entries into
+// CSR in list order for the Taubin and normals kernels.
+#include <cub/cub.cuh>
+#include "egt_internal.cuh"
+
+namespace egt {
+namespace {
+
+constexpr int kWarps = 8;
+
+template <int S>
+__global__ void __launch_bounds__(kWarps * 32) k_egt(const float4* __restrict__ p4, int* __restrict__ lists,
+                                                     int n, int k, float alpha, int* __restrict__ counts) {
+    const int lane = threadIdx.x & 31;
+    const int q = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    if (q >= n) return;
+    const float4 p = p4[q];
+    int nb[S];
+    float4 v[S];
+    bool keep[S], test[S];
+    float ax[S], ay[S], az[S], px[S], py[S], pz[S], qx[S], qy[S], qz[S], tx[S], ty[S], tz[S], dd[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        nb[s] = t < k ? lists[(size_t)q * k + t] : -1;
+        v[s] = nb[s] >= 0 ? p4[nb[s]] : make_float4(0.f, 0.f, 0.f, 0.f);
+        keep[s] = nb[s] != -1;
+        test[s] = false;
+        if (keep[s]) {
+            const float xi = v[s].x, yi = v[s].y, zi = v[s].z;
+            const float xo = __fmul_rn(0.5f, __fadd_rn(xi, p.x));
+            const float yo = __fmul_rn(0.5f, __fadd_rn(yi, p.y));
+            const float zo = __fmul_rn(0.5f, __fadd_rn(zi, p.z));
+            const float d = __fdiv_rn(__fsqrt_rn(fs_dist3(xi, yi, zi, p.x, p.y, p.z)), 2.0f);
+            float ex = __fsub_rn(xi, p.x), ey = __fsub_rn(yi, p.y), ez = __fsub_rn(zi, p.z);
+            const float len = __fsqrt_rn(fs_sq3(ex, ey, ez));
+            if (!((double)d < 1e-6) && !((double)len < 1e-6)) {
+                test[s] = true;
+                // x axis
+                ex = __fdiv_rn(ex, len); ey = __fdiv_rn(ey, len); ez = __fdiv_rn(ez, len);
+                // y axis: unit vector perpendicular to x (EGT_CUDA.cu:61-95)
+                float m = fabsf(ex);
+                int ci = 0;
+                if (m < fabsf(ey)) { ci = 1; m = fabsf(ey); }
+                if (m < fabsf(ez)) ci = 2;
+                float ux = 1.0f, uy = 1.0f, uz = 1.0f;
+                if (ci == 0) ux = __fdiv_rn(__fsub_rn(-ey, ez), ex);
+                else if (ci == 1) uy = __fdiv_rn(__fsub_rn(-ex, ez), ey);
+                else uz = __fdiv_rn(__fsub_rn(-ex, ey), ez);
+                const float ul = __fsqrt_rn(fs_sq3(ux, uy, uz));
+                ux = __fdiv_rn(ux, ul); uy = __fdiv_rn(uy, ul); uz = __fdiv_rn(uz, ul);
+                // z axis = x cross y, normalised
+                float wx = fs_cross1(ey, uz, uy, ez);
+                float wy = fs_cross1(ux, ez, ex, uz);
+                float wz = fs_cross1(ex, uy, ux, ey);
+                const float wl = __fsqrt_rn(fs_sq3(wx, wy, wz));
+                wx = __fdiv_rn(wx, wl); wy = __fdiv_rn(wy, wl); wz = __fdiv_rn(wz, wl);
+                ax[s] = ex; ay[s] = ey; az[s] = ez;
+                px[s] = ux; py[s] = uy; pz[s] = uz;
+                qx[s] = wx; qy[s] = wy; qz[s] = wz;
+                tx[s] = -fs_affine(ex, ey, ez, 0.0f, xo, yo, zo);
+                ty[s] = -fs_affine(ux, uy, uz, 0.0f, xo, yo, zo);
+                tz[s] = -fs_affine(wx, wy, wz, 0.0f, xo, yo, zo);
+                dd[s] = __fmul_rn(d, d);
+            }
+        }
+    }
+    const float aa = __fmul_rn(alpha, alpha);
+    // last slot index that still has something to test
+    int hi = -1;
+#pragma unroll
+    for (int s = 0; s < S; s++)
+        if (test[s]) hi = lane + 32 * s;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    for (int jp = 0; jp < hi; jp++) {
+        const int sl = jp & 31, ss = jp >> 5;
+        int bn = nb[0];
+        float4 bv = v[0];
+#pragma unroll
+        for (int s = 1; s < S; s++)
+            if (ss == s) { bn = nb[s]; bv = v[s]; }
+        bn = __shfl_sync(0xffffffffu, bn, sl);
+        if (bn < 0) continue;  // uniform
+        const float ux = __shfl_sync(0xffffffffu, bv.x, sl);
+        const float uy = __shfl_sync(0xffffffffu, bv.y, sl);
+        const float uz = __shfl_sync(0xffffffffu, bv.z, sl);
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            const int t = lane + 32 * s;
+            if (test[s] && keep[s] && jp < t) {
+                const float lx = fs_affine(ax[s], ay[s], az[s], tx[s], ux, uy, uz);
+                const float ly = fs_affine(px[s], py[s], pz[s], ty[s], ux, uy, uz);
+                const float lz = fs_affine(qx[s], qy[s], qz[s], tz[s], ux, uy, uz);
+                if (fs_ellipsoid(lx, ly, lz, aa) < dd[s]) keep[s] = false;
+            }
+        }
+    }
+    int cnt = 0;
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        if (t < k && nb[s] != -1 && !keep[s]) lists[(size_t)q * k + t] = -1;
+        cnt += __popc(__ballot_sync(0xffffffffu, keep[s]));
+    }
+    if (lane == 0) counts[q] = cnt;
+}
+
+// Packs the kept entries of each row, in list order, into CSR columns.
+template <int S>
+__global__ void __launch_bounds__(kWarps * 32) k_compact(const int* __restrict__ lists, int n, int k,
+                                                         const int* __restrict__ off, int* __restrict__ col) {
+    const int lane = threadIdx.x & 31;
+    const int q = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    if (q >= n) return;
+    int base = off[q];
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        const int v = t < k ? lists[(size_t)q * k + t] : -1;
+        const unsigned m = __ballot_sync(0xffffffffu, v >= 0);
+        if (v >= 0) col[base + __popc(m & ((1u << lane) - 1u))] = v;
+        base += __popc(m);
+    }
+}
+
+__global__ void k_count_valid(const int* __restrict__ lists, int n, int k, int* __restrict__ counts) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = 0;
+    for (int j = 0; j < k; j++) c += lists[(size_t)i * k + j] >= 0;
+    counts[i] = c;
+}
+
+template <int S>
+egt_status launch_egt(egt_handle* h, float alpha, int* counts) {
+    const unsigned G = (unsigned)((h->n + kWarps - 1) / kWarps);
+    k_egt<S><<<G, kWarps * 32, 0, h->stream>>>(h->p4, h->lists, (int)h->n, h->k, alpha, counts);
+    EGT_LAUNCH_CHECK();
+    return EGT_OK;
+}
+
+template <int S>
+egt_status launch_compact(egt_handle* h) {
+    const unsigned G = (unsigned)((h->n + kWarps - 1) / kWarps);
+    k_compact<S><<<G, kWarps * 32, 0, h->stream>>>(h->lists, (int)h->n, h->k, h->csr_off, h->csr_col);
+    EGT_LAUNCH_CHECK();
+    return EGT_OK;
+}
+
+}  // namespace
+
+// Builds the CSR view of the current lists (no filtering).
+static egt_status build_csr(egt_handle* h, int* counts) {
+    cudaStream_t st = h->stream;
+    const int64_t n = h->n;
+    size_t cub_scan = 0;
+    EGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, cub_scan, (int*)nullptr, (int*)nullptr, (int)(n + 1), st));
+    void* tmp = nullptr;
+    EGT_TRY(scratch_reserve(h, cub_scan, &tmp));
+    if (!h->csr_off) EGT_CUDA_TRY(cudaMalloc(&h->csr_off, sizeof(int) * (n + 1)));
+    // counts has n+1 entries, the last one zero: the exclusive sum's last element is nnz
+    EGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, cub_scan, counts, h->csr_off, (int)(n + 1), st));
+    int nnz = 0;
+    EGT_CUDA_TRY(cudaMemcpyAsync(&nnz, h->csr_off + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EGT_CUDA_TRY(cudaStreamSynchronize(st));
+    h->nnz = nnz;
+    if (h->csr_cap < nnz || !h->csr_col) {
+        if (h->csr_col) EGT_CUDA_TRY(cudaFree(h->csr_col));
+        h->csr_col = nullptr;
+        EGT_CUDA_TRY(cudaMalloc(&h->csr_col, sizeof(int) * std::max<int64_t>(nnz, 1)));
+        h->csr_cap = std::max<int64_t>(nnz, 1);
+    }
+    const int k = h->k;
+    if (k <= 32) EGT_TRY(launch_compact<1>(h));
+    else if (k <= 64) EGT_TRY(launch_compact<2>(h));
+    else if (k <= 128) EGT_TRY(launch_compact<4>(h));
+    else EGT_TRY(launch_compact<8>(h));
+    h->have_csr = true;
+    return EGT_OK;
+}
+
+egt_status run_egt(egt_handle* h, float alpha) {
+    if (!h->lists || h->k <= 0) { set_error("egt_filter: no neighbour lists (call egt_knn first)"); return EGT_ERR_STATE; }
+    cudaStream_t st = h->stream;
+    const int64_t n = h->n;
+    int* counts = nullptr;
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&counts, sizeof(int) * (n + 1), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(counts + n, 0, sizeof(int), st));
+    EGT_CUDA_TRY(cudaEventRecord(h->ev[4], st));
+    const int k = h->k;
+    egt_status s;
+    if (k <= 32) s = launch_egt<1>(h, alpha, counts);
+    else if (k <= 64) s = launch_egt<2>(h, alpha, counts);
+    else if (k <= 128) s = launch_egt<4>(h, alpha, counts);
+    else s = launch_egt<8>(h, alpha, counts);
+    if (s == EGT_OK) s = build_csr(h, counts);
+    EGT_CUDA_TRY(cudaEventRecord(h->ev[5], st));
+    cudaFreeAsync(counts, st);
+    return s;
+}
+
+// CSR of the unfiltered lists (used when Taubin/normals run without EGT).
+egt_status ensure_csr(egt_handle* h) {
+    if (h->have_csr) return EGT_OK;
+    cudaStream_t st = h->stream;
+    const int64_t n = h->n;
+    int* counts = nullptr;
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&counts, sizeof(int) * (n + 1), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(counts + n, 0, sizeof(int), st));
+    k_count_valid<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(h->lists, (int)n, h->k, counts);
+    EGT_LAUNCH_CHECK();
+    egt_status s = build_csr(h, counts);
+    cudaFreeAsync(counts, st);
+    return s;
+}
+
+}  // namespace egt

@@ -1,0 +1,126 @@
+// Warp-cooperative sorted neighbour list with the reference's insertion rule.
+//
+// The list of a query is held in registers across the 32 lanes of a warp:
+// slot t lives in lane t % 32, register t / 32 (S registers per lane, k <= 32*S).
+// insert() reproduces newNeighborSearch::appendDistanceGrid
+// (GridKNNCuda.cu:311-339) exactly:
+//   * admit only if d < list[k-1] (the list is pre-filled with 1e10, so this is
+//     "always" while the list is not full, and strict at the k-th slot);
+//   * reject an index already among the first `counter` slots;
+//   * insert at FindPosition(list, d, 0, counter-1) (GridKNNCuda.cu:126-143): the
+//     binary search returns the slot of the first equal element it meets, or
+//     the insertion point -- equal distances therefore land where that search
+//     lands, not simply after the existing ones;
+//   * shift the tail down by one, dropping slot k-1 when the list is full.
+// All lanes call insert() with the same (d, p): control flow stays uniform.
+#pragma once
+#include "egt_internal.cuh"
+
+namespace egt {
+
+template <int S>
+struct WarpList {
+    float dist[S];
+    int idx[S];
+    int counter;  // number of filled slots (uniform)
+    float kth;    // value of slot k-1 (uniform): 1e10 until the list is full
+    int k;
+
+    __device__ __forceinline__ void init(int k_) {
+#pragma unroll
+        for (int s = 0; s < S; s++) { dist[s] = 1e10f; idx[s] = -1; }
+        counter = 0;
+        kth = 1e10f;
+        k = k_;
+    }
+
+    __device__ __forceinline__ float fetch_dist(int t) const {
+        float v = dist[0];
+#pragma unroll
+        for (int s = 1; s < S; s++)
+            if ((t >> 5) == s) v = dist[s];
+        return __shfl_sync(0xffffffffu, v, t & 31);
+    }
+
+    __device__ __forceinline__ void insert(float d, int p, int lane) {
+        if (!(d < kth)) return;
+        // dedup among the filled slots
+        bool dup = false, eq = false;
+        unsigned lt = 0;
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            const int t = lane + 32 * s;
+            const bool live = t < counter;
+            dup |= live && idx[s] == p;
+            eq |= live && dist[s] == d;
+            lt += __popc(__ballot_sync(0xffffffffu, live && dist[s] < d));
+        }
+        if (__any_sync(0xffffffffu, dup)) return;
+        int pos;
+        if (!__any_sync(0xffffffffu, eq)) {
+            pos = (int)lt;  // no equal element: FindPosition returns the insertion point
+        } else {
+            int low = 0, high = counter - 1;
+            pos = -1;
+            while (low <= high) {  // at most log2(k)+1 iterations
+                const int mid = low + (high - low) / 2;
+                const float a = fetch_dist(mid);
+                if (a == d) { pos = mid; break; }
+                if (a < d) low = mid + 1;
+                else high = mid - 1;
+            }
+            if (pos < 0) pos = low + (high - low) / 2;
+        }
+        // previous slot values (t-1) for the shift, taken before any update
+        float pd[S];
+        int pi[S];
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            float up_d = __shfl_up_sync(0xffffffffu, dist[s], 1);
+            int up_i = __shfl_up_sync(0xffffffffu, idx[s], 1);
+            float wrap_d = __shfl_sync(0xffffffffu, s > 0 ? dist[s > 0 ? s - 1 : 0] : 0.f, 31);
+            int wrap_i = __shfl_sync(0xffffffffu, s > 0 ? idx[s > 0 ? s - 1 : 0] : 0, 31);
+            pd[s] = lane == 0 ? wrap_d : up_d;
+            pi[s] = lane == 0 ? wrap_i : up_i;
+        }
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            const int t = lane + 32 * s;
+            if (t < k) {
+                if (t == pos) { dist[s] = d; idx[s] = p; }
+                else if (t > pos) { dist[s] = pd[s]; idx[s] = pi[s]; }
+            }
+        }
+        counter = counter == k ? k : counter + 1;
+        kth = fetch_dist(k - 1);
+    }
+};
+
+// Locate cell (cx,cy,cz) of a level: returns [start,end) into the level's
+// order array, or start == end == -1 when the cell is empty / out of range.
+__device__ __forceinline__ int2 find_cell(const LevelDev& L, int cx, int cy, int cz) {
+    const int B = L.B;
+    if (cx < 0 || cx >= B || cy < 0 || cy >= B || cz < 0 || cz >= B) return make_int2(-1, -1);
+    const int2 rr = L.row_range[cy + cz * B];
+    int lo = rr.x, hi = rr.y;
+    while (lo < hi) {  // at most log2(B)+1 iterations
+        const int mid = (lo + hi) >> 1;
+        if (L.cell_x[mid] < cx) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo < rr.y && L.cell_x[lo] == cx) return make_int2(L.cell_start[lo], L.cell_start[lo + 1]);
+    return make_int2(-1, -1);
+}
+
+// Shell order of GRIDCUDAKNNSELF_COMPACT for offset 1 (GridKNNCuda.cu:2480-2551).
+__constant__ static const signed char kShell[26][3] = {
+    {0, 0, -1}, {0, 0, 1},
+    {0, -1, 0}, {0, 1, 0},
+    {-1, 0, 0}, {1, 0, 0},
+    {-1, -1, 0}, {-1, 1, 0}, {1, -1, 0}, {1, 1, 0},
+    {-1, 0, -1}, {-1, 0, 1}, {1, 0, -1}, {1, 0, 1},
+    {0, -1, -1}, {0, -1, 1}, {0, 1, -1}, {0, 1, 1},
+    {-1, -1, -1}, {-1, -1, 1}, {-1, 1, -1}, {-1, 1, 1}, {1, -1, -1}, {1, -1, 1}, {1, 1, -1}, {1, 1, 1},
+};
+
+}  // namespace egt

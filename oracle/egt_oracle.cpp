@@ -14,6 +14,7 @@
 //   perm       sorted slot -> original index, int32 [n]
 //   lists      sorted-space neighbour lists, int32 [n*k], -1 padded
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -525,6 +526,36 @@ int orc_knn(const float* xyz, int n, int k, int* lists, float* pos, int* perm, f
     ext[0] = g.mn; ext[1] = g.mx;
     if (visited_total) *visited_total = visited_sum;
     return invalid_count;
+}
+
+// Timed sample of the grid kNN for the CPU baseline: builds the full grid
+// (normalisation, cell sort, 8 levels) and answers every `stride`-th query.
+// Returns the wall times of both phases (steady_clock, seconds).
+void orc_knn_timed(const float* xyz, int n, int k, int stride, double* t_build, double* t_query) {
+    auto t0 = std::chrono::steady_clock::now();
+    Grid g;
+    build_grid(xyz, n, g, kLevels);
+    float thres = 1e8f;
+    thres /= (g.mx - g.mn);
+    thres *= thres;
+    auto t1 = std::chrono::steady_clock::now();
+    long long sink = 0;
+#pragma omp parallel reduction(+ : sink)
+    {
+        std::vector<float> dist(k);
+        std::vector<int> idx(k);
+#pragma omp for schedule(dynamic, 64)
+        for (int q = 0; q < n; q += stride) {
+            int counter;
+            bool invalid;
+            long long visited = 0;
+            knn_query(g, q, k, thres, dist.data(), idx.data(), counter, invalid, visited);
+            sink += idx[0];
+        }
+    }
+    auto t2 = std::chrono::steady_clock::now();
+    *t_build = std::chrono::duration<double>(t1 - t0).count();
+    *t_query = std::chrono::duration<double>(t2 - t1).count() + (sink == 42 ? 1e-300 : 0.0);
 }
 
 // Mesh 1-ring lists of GridMeshCuda (GridMeshCuda1.cu:314-511).  Each vertex

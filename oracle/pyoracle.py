@@ -43,6 +43,7 @@ def lib():
         L.orc_orient.argtypes = [i32, i32, vp, vp, vp]
         L.orc_output.argtypes = [vp, vp, vp, i32, vp]
         L.orc_bruteforce.argtypes = [vp, i32, i32, vp, vp]
+        L.orc_knn_timed.argtypes = [vp, i32, i32, i32, vp, vp]
         _lib = L
     return _lib
 
@@ -145,3 +146,11 @@ def bruteforce(pos: np.ndarray, k: int):
     d = np.empty((n, k), np.float32)
     lib().orc_bruteforce(_p(pos), n, k, _p(lists), _p(d))
     return lists, d
+
+
+def knn_timed(xyz: np.ndarray, k: int, stride: int):
+    """(t_build, t_query) seconds for the grid build plus every stride-th query."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+    tb, tq = C.c_double(0), C.c_double(0)
+    lib().orc_knn_timed(_p(xyz), xyz.shape[0], k, stride, C.byref(tb), C.byref(tq))
+    return tb.value, tq.value

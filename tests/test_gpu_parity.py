@@ -1,0 +1,174 @@
+"""GPU parity: the sm_100a kernels, called through the C ABI, against the
+reference's own outputs (golden fixtures) and the CPU oracle.
+
+Integer/index results (kNN lists, EGT lists, permutation) must be
+bit-identical.  Positions: the Taubin kernel evaluates the reference's
+expression with the same fused multiply-adds and CUDA's expf, so its result is
+compared bit-for-bit against the reference, and within 1e-6 of the bounding-box
+diagonal against the FP64 oracle.  Normals: within 0.1 degrees of the FP64
+oracle, and oriented with the reference's sign.
+"""
+import numpy as np
+import pytest
+
+from golden_util import FULL, MESH_FULL, bbox_diag, load, regen, sha
+from multigpuegtsmoothing_b200 import datagen
+
+pytestmark = pytest.mark.gpu
+
+
+def cloud(capi, xyz, k, cfg=None):
+    g = capi.GridStructure(xyz, config=cfg)
+    g.GRIDCUDAKNNSELF_COMPACT(k)
+    return g
+
+
+@pytest.mark.parametrize("name", FULL)
+def test_knn_egt_taubin_output_match_reference(capi, oracle, name):
+    d, m = load(name)
+    g = cloud(capi, d["in_xyz"], m["k"])
+    assert np.array_equal(g.GetOriginalRefIndexes(), d["ref_perm"])
+    assert np.array_equal(g.sorted_positions(), d["ref_pos_in"])
+    assert np.float32(g.GetMinExtent()) == d["ref_extents"][0]
+    assert np.float32(g.GetMaxExtent()) == d["ref_extents"][1]
+    assert np.array_equal(g.sorted_lists(), d["ref_knn_raw"])
+    capi.EGT_CUDA(g).PerformSmoothing(m["iters"], 0.63, -0.64, m["alpha"])
+    assert np.array_equal(g.sorted_lists(), d["ref_knn_egt"])
+    pos = g.sorted_positions()
+    # smoothed positions: within 1e-6 of the bbox diagonal of the reference's
+    # FP32 result and of the FP64 oracle (original units)
+    scale = float(d["ref_extents"][1]) - float(d["ref_extents"][0])
+    tol = 1e-6 * bbox_diag(d["in_xyz"])
+    assert np.abs(pos - d["ref_pos_out"]).max() * scale <= tol
+    p64 = oracle.taubin_f64(d["ref_pos_in"], d["ref_knn_egt"], m["iters"])
+    assert np.abs(pos - p64).max() * scale <= tol
+    # the output gather itself is exact: check it on the GPU's own positions
+    x, y, z = capi.getOutputPoints(g)
+    want = oracle.output(pos, d["ref_perm"], d["ref_extents"])
+    assert np.array_equal(np.stack([x, y, z]), want)
+
+
+@pytest.mark.parametrize("name", MESH_FULL)
+def test_mesh_matches_reference(capi, name):
+    d, m = load(name)
+    g = capi.GridMeshCuda(d["in_xyz"], d["in_tris"])
+    g.GetNeighborsFromTriangles(m["k"])
+    assert np.array_equal(g.GetOriginalRefIndexes(), d["ref_perm"])
+    got = g.sorted_lists()
+    assert np.array_equal(got, d["ref_knn_raw"])
+    capi.EGT_CUDA(g).PerformSmoothing(m["iters"], 0.63, -0.64, m["alpha"])
+    assert np.array_equal(g.sorted_lists(), d["ref_knn_egt"])
+    scale = float(d["ref_extents"][1]) - float(d["ref_extents"][0])
+    assert np.abs(g.sorted_positions() - d["ref_pos_out"]).max() * scale <= 1e-6 * bbox_diag(d["in_xyz"])
+
+
+@pytest.mark.parametrize("name", ["ref_sphere_c1", "ref_torus_c2"])
+def test_full_size_configs_match_reference(capi, oracle, name):
+    d, m = load(name)
+    dg = m["digests"]
+    xyz, tris = regen(m)
+    if tris is None:
+        g = cloud(capi, xyz, m["k"])
+    else:
+        g = capi.GridMeshCuda(xyz, tris)
+        g.GetNeighborsFromTriangles(m["k"])
+    assert sha(g.GetOriginalRefIndexes()) == dg["ref_perm"]
+    assert sha(g.sorted_lists()) == dg["ref_knn_raw"]
+    capi.EGT_CUDA(g).PerformSmoothing(m["iters"], 0.63, -0.64, m["alpha"])
+    lists = g.sorted_lists()
+    assert sha(lists) == dg["ref_knn_egt"]
+    pos = g.sorted_positions()
+    rows = d["rows"]
+    p0 = oracle.knn(xyz, m["k"]) if tris is None else oracle.mesh_1ring(xyz, tris, m["k"])
+    scale = float(p0["ext"][1]) - float(p0["ext"][0])
+    tol = 1e-6 * bbox_diag(xyz)
+    # FP32 smoothing against the reference's FP32 result and the FP64 oracle
+    assert np.abs(pos[:, rows] - d["ref_pos_out_cols"]).max() * scale <= tol
+    p64 = oracle.taubin_f64(p0["pos"], lists, m["iters"])
+    assert np.abs(pos - p64).max() * scale <= tol
+
+
+@pytest.mark.parametrize("n,k,seed", [(1000, 1, 1), (5000, 10, 2), (20000, 33, 3), (8000, 64, 4),
+                                      (6000, 100, 5), (3000, 200, 6)])
+def test_knn_matches_oracle_random(capi, oracle, n, k, seed):
+    xyz = datagen.sphere_cloud(n, 0.02, seed)
+    g = cloud(capi, xyz, k)
+    r = oracle.knn(xyz, k)
+    assert np.array_equal(g.sorted_lists(), r["lists"])
+    assert g.timings()["invalid_queries"] == r["invalid"]
+
+
+def test_knn_superquadric_subset(capi, oracle):
+    xyz = datagen.superquadrics(200_000, seed=31)
+    g = cloud(capi, xyz, 40)
+    r = oracle.knn(xyz, 40)
+    assert np.array_equal(g.sorted_lists(), r["lists"])
+    capi.EGT_CUDA(g).Filter(0.65)
+    assert np.array_equal(g.sorted_lists(), oracle.egt(r["pos"], r["lists"], 0.65))
+
+
+def test_edge_cases(capi, oracle):
+    # a single point: no neighbours, the row is invalid
+    g = cloud(capi, np.zeros((1, 3), np.float32), 4)
+    assert (g.sorted_lists() == -1).all()
+    # fewer points than k: every row invalid (hierarchy exhausted)
+    xyz = datagen.sphere_cloud(20, 0.01, 7)
+    g = cloud(capi, xyz, 40)
+    assert (g.sorted_lists() == -1).all()
+    # all points identical: one cell; with a small cell cap every query is invalid
+    same = np.ones((300, 3), np.float32)
+    g = cloud(capi, same, 8, capi.default_config(max_points_in_cell=100))
+    assert (g.sorted_lists() == -1).all()
+    g = cloud(capi, same, 8)
+    r = oracle.knn(same, 8)
+    assert np.array_equal(g.sorted_lists(), r["lists"])
+    # exact duplicates and ties
+    d, m = load("ref_dups")
+    g = cloud(capi, d["in_xyz"], 5)
+    assert np.array_equal(g.sorted_lists(), oracle.knn(d["in_xyz"], 5)["lists"])
+
+
+def test_bad_arguments(capi):
+    with pytest.raises(capi.EgtError):
+        cloud(capi, datagen.sphere_cloud(100, 0.01, 8), 0)
+    g = capi.GridStructure(datagen.sphere_cloud(100, 0.01, 8))
+    with pytest.raises(capi.EgtError):
+        capi.EGT_CUDA(g).Filter(0.65)  # no lists yet
+    with pytest.raises(capi.EgtError):
+        capi.GridStructure(datagen.sphere_cloud(100, 0.01, 8), bucketCount=512)
+    with pytest.raises(capi.EgtError):
+        capi.GridStructure(datagen.sphere_cloud(100, 0.01, 8), num_cards=2)
+
+
+def test_deterministic(capi):
+    xyz = datagen.superquadrics(100_000, seed=9)
+    outs = []
+    for _ in range(2):
+        g = cloud(capi, xyz, 40)
+        capi.EGT_CUDA(g).PerformSmoothing(5, 0.63, -0.64, 0.65)
+        nx, ny, nz = capi.Normal_CUDA(g).GetNormals()
+        outs.append((g.sorted_lists().tobytes(), g.sorted_positions().tobytes(), nx.tobytes() + ny.tobytes()))
+    assert outs[0] == outs[1]
+
+
+def test_knn_host_original_order(capi, oracle):
+    xyz = datagen.sphere_cloud(3000, 0.01, 10)
+    g = cloud(capi, xyz, 12)
+    got = g.GetKNNIndexes()
+    r = oracle.knn(xyz, 12)
+    perm = r["perm"]
+    want = np.full_like(r["lists"], -1)
+    valid = r["lists"] >= 0
+    mapped = np.where(valid, perm[np.clip(r["lists"], 0, None)], -1)
+    want[perm] = mapped
+    assert np.array_equal(got, want)
+
+
+def test_superquadrics_4m_digest(capi):
+    d, m = load("ref_superquadrics_4m")
+    dg = m["digests"]
+    xyz, _ = regen(m)
+    g = cloud(capi, xyz, m["k"])
+    assert sha(g.sorted_lists()) == dg["ref_knn_raw"]
+    capi.EGT_CUDA(g).Filter(m["alpha"])
+    assert sha(g.sorted_lists()) == dg["ref_knn_egt"]

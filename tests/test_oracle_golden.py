@@ -1,0 +1,86 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures).
+
+The fixtures were produced by running the unmodified reference (built from its
+sources, tests/golden/make_golden.py).  These tests pin the oracle: the kNN
+lists, the EGT-filtered lists, the cell-sorted normalised positions, the
+permutation, the extents and the output gather must be bit-identical; the
+FP32 Taubin result may differ only by CUDA's expf vs the host's expf, and both
+must sit within 1e-6 of the bounding-box diagonal of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from golden_util import FULL, MESH_FULL, bbox_diag, load, regen, sha
+
+
+@pytest.mark.parametrize("name", FULL)
+def test_cloud_small_bitexact(oracle, name):
+    d, m = load(name)
+    r = oracle.knn(d["in_xyz"], m["k"])
+    assert np.array_equal(r["perm"], d["ref_perm"])
+    assert np.array_equal(r["ext"], d["ref_extents"])
+    assert np.array_equal(r["pos"], d["ref_pos_in"])
+    assert np.array_equal(r["lists"], d["ref_knn_raw"])
+    e = oracle.egt(d["ref_pos_in"], d["ref_knn_raw"], m["alpha"])
+    assert np.array_equal(e, d["ref_knn_egt"])
+    out = oracle.output(d["ref_pos_out"], d["ref_perm"], d["ref_extents"])
+    assert np.array_equal(out, d["ref_out_xyz"])
+
+
+@pytest.mark.parametrize("name", MESH_FULL)
+def test_mesh_small_bitexact(oracle, name):
+    d, m = load(name)
+    r = oracle.mesh_1ring(d["in_xyz"], d["in_tris"], m["k"])
+    assert np.array_equal(r["perm"], d["ref_perm"])
+    assert np.array_equal(r["pos"], d["ref_pos_in"])
+    assert np.array_equal(r["lists"], d["ref_knn_raw"])
+    e = oracle.egt(d["ref_pos_in"], d["ref_knn_raw"], m["alpha"])
+    assert np.array_equal(e, d["ref_knn_egt"])
+
+
+@pytest.mark.parametrize("name", FULL + MESH_FULL)
+def test_taubin_tolerance(oracle, name):
+    d, m = load(name)
+    p32 = oracle.taubin_f32(d["ref_pos_in"], d["ref_knn_egt"], m["iters"])
+    p64 = oracle.taubin_f64(d["ref_pos_in"], d["ref_knn_egt"], m["iters"])
+    ext = d["ref_extents"]
+    scale = float(ext[1]) - float(ext[0])
+    diag = bbox_diag(d["in_xyz"])
+    tol = 1e-6 * diag  # north-star tolerance for smoothed positions
+    assert np.abs(d["ref_pos_out"] - p64).max() * scale <= tol
+    assert np.abs(p32 - p64).max() * scale <= tol
+    # FP32 mirror vs reference: only expf rounding differs
+    assert np.abs(p32 - d["ref_pos_out"]).max() < 1e-6
+
+
+@pytest.mark.parametrize("name", ["ref_sphere_c1", "ref_torus_c2"])
+def test_full_size_digests(oracle, name):
+    d, m = load(name)
+    dg = m["digests"]
+    xyz, tris = regen(m)
+    assert sha(xyz) == dg["in_xyz"], "generator changed: regenerate the fixtures"
+    r = oracle.knn(xyz, m["k"]) if tris is None else oracle.mesh_1ring(xyz, tris, m["k"])
+    assert sha(r["perm"]) == dg["ref_perm"]
+    assert sha(r["pos"]) == dg["ref_pos_in"]
+    assert sha(r["lists"]) == dg["ref_knn_raw"]
+    rows = d["rows"]
+    assert np.array_equal(r["lists"][rows], d["ref_knn_raw_rows"])
+    e = oracle.egt(r["pos"], r["lists"], m["alpha"])
+    assert sha(e) == dg["ref_knn_egt"]
+    p64 = oracle.taubin_f64(r["pos"], e, m["iters"])
+    scale = float(r["ext"][1]) - float(r["ext"][0])
+    err = np.abs(p64[:, rows] - d["ref_pos_out_cols"]).max() * scale
+    assert err <= 1e-6 * bbox_diag(xyz)
+
+
+def test_superquadrics_4m_digest(oracle):
+    """All 4,000,000 kNN rows and EGT rows of the 4M-point workload."""
+    d, m = load("ref_superquadrics_4m")
+    dg = m["digests"]
+    xyz, _ = regen(m)
+    assert sha(xyz) == dg["in_xyz"]
+    r = oracle.knn(xyz, m["k"])
+    assert sha(r["lists"]) == dg["ref_knn_raw"]
+    assert sha(r["pos"]) == dg["ref_pos_in"]
+    e = oracle.egt(r["pos"], r["lists"], m["alpha"])
+    assert sha(e) == dg["ref_knn_egt"]
