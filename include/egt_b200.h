@@ -129,6 +129,21 @@ egt_status egt_get_timings(egt_handle* h, egt_timings* t);
  * until the next call on the handle): offsets [n+1], cols [nnz]. */
 egt_status egt_get_csr(egt_handle* h, const int** offsets, const int** cols, int64_t* nnz);
 
+/* Taubin lambda/mu smoothing that allocates no device memory, for callers that
+ * cannot allocate: hosts whose single allocator owns all GPU memory, real-time
+ * loops that cannot afford cudaMalloc's implicit synchronisation, and code
+ * recorded into a CUDA graph.  No counterpart in the reference.
+ * pos_in/pos_out: n float4 (x,y,z,w) in device memory (may alias);
+ * csr_off [n+1] / csr_col: the neighbourhoods (e.g. from egt_get_csr).
+ * The intermediate positions live in a fixed device array of 2^20 float4
+ * (16 MB, held by every GPU that loads the library); n above 2^20 is rejected
+ * with EGT_ERR_ARG.  The first call on a device resolves that array's device
+ * address (cudaGetSymbolAddress), so make it before any stream capture.  All
+ * calls share the array: calls that may overlap on the GPU race and must be
+ * serialised by the caller. */
+egt_status egt_taubin_noalloc(const float* pos_in, float* pos_out, const int* csr_off, const int* csr_col,
+                              int64_t n, int iters, float lambda, float mu, void* stream);
+
 /* Copies bytes from device memory (e.g. a pointer from egt_get_views) to host
  * memory after synchronising the handle's stream.  No reference counterpart:
  * lets hosts without their own CUDA runtime binding read the device views. */

@@ -94,6 +94,7 @@ def lib() -> C.CDLL:
             "egt_copy_to_host": (i32, [vp, vp, vp, i64]),
             "egt_update_points_device": (i32, [vp, vp, vp]),
             "egt_kernel_launches": (i64, []),
+            "egt_taubin_noalloc": (i32, [vp, vp, vp, vp, i64, i32, f32, f32, vp]),
             "egt_destroy": (None, [vp]),
         }
         for name, (res, args) in sigs.items():
