@@ -230,7 +230,8 @@ def run_b200(args, world, rank, local):
     # Taubin: EGT filter once, then ITERS lambda/mu iterations in one CUDA graph
     egt = capi.EGT_CUDA(g)
     egt.Filter(ALPHA)
-    t_egt = g.timings()["egt_ms"]
+    tmf = g.timings()
+    t_egt, t_egt_kernel = tmf["egt_ms"], tmf["egt_kernel_ms"]
     nnz = g.timings()["csr_nnz"]
     egt.Taubin(ITERS)  # warm-up (graph capture path)
     torch.cuda.synchronize()
@@ -274,6 +275,7 @@ def run_b200(args, world, rank, local):
                        "n_points": n, "k": K, "parallelism": f"replicas{world}",
                        "l2": "per-step footprint > L2 (n*k*4 = 640 MB of lists written per step)"},
             "stages_ms": {"grid_build": build_ms, "knn_query": knn_ms, "egt_filter": t_egt,
+                          "egt_filter_kernel": t_egt_kernel,
                           "taubin_300_iters": taubin_ms},
             "taubin_iters_per_s": ITERS / (taubin_ms * 1e-3),
             "taubin_roofline": {"bound": "hbm", "achieved": taubin_gbs, "peak": peak, "unit": "GB/s",

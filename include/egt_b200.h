@@ -71,6 +71,7 @@ typedef struct egt_timings {
     int64_t normals_fp64;    /* points whose normal was re-solved in FP64 */
     int64_t msf_edges;       /* edges of the orientation spanning forest */
     int components;          /* orientation components (trees with >= 1 edge) */
+    float egt_kernel_ms;     /* the EGT filter kernel alone (egt_ms also packs the CSR) */
 } egt_timings;
 
 void egt_default_config(egt_config* cfg);

@@ -54,7 +54,8 @@ class Timings(C.Structure):
     _fields_ = [("grid_ms", C.c_float), ("knn_ms", C.c_float), ("egt_ms", C.c_float), ("taubin_ms", C.c_float),
                 ("normals_ms", C.c_float), ("orient_ms", C.c_float), ("output_ms", C.c_float),
                 ("levels_used", C.c_int), ("invalid_queries", C.c_int64), ("csr_nnz", C.c_int64),
-                ("normals_fp64", C.c_int64), ("msf_edges", C.c_int64), ("components", C.c_int)]
+                ("normals_fp64", C.c_int64), ("msf_edges", C.c_int64), ("components", C.c_int),
+                ("egt_kernel_ms", C.c_float)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

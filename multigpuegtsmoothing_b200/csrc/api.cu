@@ -46,7 +46,7 @@ void bind_stream(egt_handle* h, void* stream) { h->stream = (cudaStream_t)stream
 void free_handle(egt_handle* h) {
     if (!h) return;
     cudaSetDevice(h->cfg.device);
-    auto F = [](void* p) { if (p) cudaFree(p); };
+    auto F = [h](void* p) { dev_free(h, p); };
     F(h->p4); F(h->p4b); F(h->x); F(h->y); F(h->z); F(h->cell0); F(h->perm); F(h->d_norm);
     for (int L = 0; L < kMaxLevels; L++) {
         F(h->lv[L].order); F(h->lv[L].cell_start); F(h->lv[L].cell_x); F(h->lv[L].row_range);
@@ -54,9 +54,26 @@ void free_handle(egt_handle* h) {
     F(h->lists); F(h->kth); F(h->qlevel); F(h->csr_off); F(h->csr_col); F(h->tris); F(h->nrm);
     F(h->d_counters); F(h->scratch.ptr);
     if (h->taubin_exec) cudaGraphExecDestroy(h->taubin_exec);
+    F(h->m_perm); F(h->m_inv); F(h->m_p); F(h->m_pb); F(h->m_off); F(h->m_col);
+    F(h->t_uni); F(h->t_loc); F(h->t_nu);
+    cudaStreamSynchronize(h->stream);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
     delete h;
+}
+
+// Keeps freed pool memory cached in the device's default memory pool.
+egt_status warm_pool(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0 || device >= 64 || done[device]) return EGT_OK;
+    cudaMemPool_t pool;
+    EGT_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t threshold = ~0ull;
+    EGT_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    done[device] = true;
+    return EGT_OK;
 }
 
 egt_status create_common(const float* xyz, bool xyz_on_device, int64_t n, const uint32_t* tris, int64_t t,
@@ -75,6 +92,7 @@ egt_status create_common(const float* xyz, bool xyz_on_device, int64_t n, const 
     }
     if (cfg.max_points_in_cell < 1) { set_error("max_points_in_cell must be >= 1"); return EGT_ERR_ARG; }
     EGT_CUDA_TRY(cudaSetDevice(cfg.device));
+    EGT_TRY(warm_pool(cfg.device));
     egt_handle* h = new egt_handle();
     h->cfg = cfg;
     h->n = n;
@@ -90,14 +108,14 @@ egt_status create_common(const float* xyz, bool xyz_on_device, int64_t n, const 
             return fail(e__ == cudaErrorMemoryAllocation ? EGT_ERR_NOMEM : EGT_ERR_CUDA); \
         }                                                                    \
     } while (0)
-    CREATE_TRY(cudaMalloc(&h->p4, sizeof(float4) * n));
-    CREATE_TRY(cudaMalloc(&h->x, sizeof(float) * n));
-    CREATE_TRY(cudaMalloc(&h->y, sizeof(float) * n));
-    CREATE_TRY(cudaMalloc(&h->z, sizeof(float) * n));
-    CREATE_TRY(cudaMalloc(&h->cell0, sizeof(uint32_t) * n));
-    CREATE_TRY(cudaMalloc(&h->perm, sizeof(int) * n));
-    CREATE_TRY(cudaMalloc(&h->d_norm, sizeof(NormParams)));
-    CREATE_TRY(cudaMalloc(&h->d_counters, sizeof(unsigned long long) * kCtrWords));
+    CREATE_TRY(dev_alloc(h, &h->p4, sizeof(float4) * n));
+    CREATE_TRY(dev_alloc(h, &h->x, sizeof(float) * n));
+    CREATE_TRY(dev_alloc(h, &h->y, sizeof(float) * n));
+    CREATE_TRY(dev_alloc(h, &h->z, sizeof(float) * n));
+    CREATE_TRY(dev_alloc(h, &h->cell0, sizeof(uint32_t) * n));
+    CREATE_TRY(dev_alloc(h, &h->perm, sizeof(int) * n));
+    CREATE_TRY(dev_alloc(h, &h->d_norm, sizeof(NormParams)));
+    CREATE_TRY(dev_alloc(h, &h->d_counters, sizeof(unsigned long long) * kCtrWords));
     CREATE_TRY(cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * kCtrWords, h->stream));
     for (auto& e : h->ev) CREATE_TRY(cudaEventCreate(&e));
     const float* dxyz = xyz;
@@ -108,7 +126,7 @@ egt_status create_common(const float* xyz, bool xyz_on_device, int64_t n, const 
         dxyz = staged;
     }
     if (tris && t > 0) {
-        CREATE_TRY(cudaMalloc(&h->tris, sizeof(uint32_t) * 3 * t));
+        CREATE_TRY(dev_alloc(h, &h->tris, sizeof(uint32_t) * 3 * t));
         CREATE_TRY(cudaMemcpyAsync(h->tris, tris, sizeof(uint32_t) * 3 * t, cudaMemcpyHostToDevice, h->stream));
     }
     egt_status s = build_grid(h, dxyz, h->is_mesh ? 1 : kMaxLevels);
@@ -164,7 +182,7 @@ egt_status egt_update_points_device(egt_handle* h, const float* xyz_dev, void* s
     EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
     bind_stream(h, stream);
     h->have_csr = false;
-    if (h->nrm) { cudaFree(h->nrm); h->nrm = nullptr; }
+    if (h->nrm) { dev_free(h, h->nrm); h->nrm = nullptr; }
     return build_grid(h, xyz_dev, kMaxLevels);
 }
 
@@ -296,9 +314,11 @@ egt_status egt_get_csr(egt_handle* h, const int** offsets, const int** cols, int
     if (!h->lists) { set_error("egt_get_csr: no neighbour lists"); return EGT_ERR_STATE; }
     EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
     EGT_TRY(ensure_csr(h));
+    int64_t m = 0;
+    EGT_TRY(csr_nnz(h, &m));
     if (offsets) *offsets = h->csr_off;
     if (cols) *cols = h->csr_col;
-    if (nnz) *nnz = h->nnz;
+    if (nnz) *nnz = m;
     return EGT_OK;
 }
 
@@ -311,13 +331,14 @@ egt_status egt_get_timings(egt_handle* h, egt_timings* t) {
     EGT_CUDA_TRY(cudaMemcpy(ctr, h->d_counters, sizeof(ctr), cudaMemcpyDeviceToHost));
     h->tm.knn_ms = elapsed_ms(h->ev[2], h->ev[3]);
     h->tm.egt_ms = elapsed_ms(h->ev[4], h->ev[5]);
+    h->tm.egt_kernel_ms = elapsed_ms(h->ev[4], h->ev[14]);
     h->tm.taubin_ms = elapsed_ms(h->ev[6], h->ev[7]);
     h->tm.normals_ms = elapsed_ms(h->ev[8], h->ev[9]);
     h->tm.orient_ms = elapsed_ms(h->ev[10], h->ev[11]);
     h->tm.output_ms = elapsed_ms(h->ev[12], h->ev[13]);
     h->tm.invalid_queries = (int64_t)ctr[kCtrInvalid];
     h->tm.levels_used = (int)ctr[kCtrMaxLevel];
-    h->tm.csr_nnz = h->nnz;
+    if (h->have_csr) EGT_TRY(csr_nnz(h, &h->tm.csr_nnz));
     h->tm.normals_fp64 = (int64_t)ctr[kCtrNormFallback];
     h->tm.msf_edges = (int64_t)ctr[kCtrMsf];
     h->tm.components = (int)ctr[kCtrComps];

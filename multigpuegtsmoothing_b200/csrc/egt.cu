@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_egt(const float4* __restrict__ 
         }
     }
     const float aa = __fmul_rn(alpha, alpha);
+    const float inv_aa = 1.0f / aa;
     // last slot index that still has something to test
     int hi = -1;
 #pragma unroll
@@ -90,6 +91,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_egt(const float4* __restrict__ 
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
     for (int jp = 0; jp < hi; jp++) {
+        if ((jp & 7) == 0) {  // stop once every slot with a pending test is decided
+            bool pending = false;
+#pragma unroll
+            for (int s = 0; s < S; s++) pending |= test[s] && keep[s] && jp < lane + 32 * s;
+            if (!__any_sync(0xffffffffu, pending)) break;
+        }
         const int sl = jp & 31, ss = jp >> 5;
         int bn = nb[0];
         float4 bv = v[0];
@@ -108,7 +115,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_egt(const float4* __restrict__ 
                 const float lx = fs_affine(ax[s], ay[s], az[s], tx[s], ux, uy, uz);
                 const float ly = fs_affine(px[s], py[s], pz[s], ty[s], ux, uy, uz);
                 const float lz = fs_affine(qx[s], qy[s], qz[s], tz[s], ux, uy, uz);
-                if (fs_ellipsoid(lx, ly, lz, aa) < dd[s]) keep[s] = false;
+                // Estimate with a reciprocal (relative error < 1e-6 of the exact
+                // expression); the exact divisions decide only near the threshold.
+                const float est = __fmaf_rn(lx, lx, __fmul_rn(__fmaf_rn(ly, ly, __fmul_rn(lz, lz)), inv_aa));
+                bool inside;
+                if (est < dd[s] * 0.99999f) inside = true;
+                else if (est > dd[s] * 1.00001f) inside = false;
+                else inside = fs_ellipsoid(lx, ly, lz, aa) < dd[s];
+                if (inside) keep[s] = false;
             }
         }
     }
@@ -166,7 +180,10 @@ egt_status launch_compact(egt_handle* h) {
 
 }  // namespace
 
-// Builds the CSR view of the current lists (no filtering).
+// Builds the CSR view of the current lists.  counts [n+1] holds the kept
+// entries per row (last element 0).  Columns are packed into a buffer of
+// capacity n*k, so no host round trip is needed for the size; nnz is read back
+// lazily (egt_get_timings / egt_get_csr).
 static egt_status build_csr(egt_handle* h, int* counts) {
     cudaStream_t st = h->stream;
     const int64_t n = h->n;
@@ -174,25 +191,35 @@ static egt_status build_csr(egt_handle* h, int* counts) {
     EGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, cub_scan, (int*)nullptr, (int*)nullptr, (int)(n + 1), st));
     void* tmp = nullptr;
     EGT_TRY(scratch_reserve(h, cub_scan, &tmp));
-    if (!h->csr_off) EGT_CUDA_TRY(cudaMalloc(&h->csr_off, sizeof(int) * (n + 1)));
-    // counts has n+1 entries, the last one zero: the exclusive sum's last element is nnz
-    EGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, cub_scan, counts, h->csr_off, (int)(n + 1), st));
-    int nnz = 0;
-    EGT_CUDA_TRY(cudaMemcpyAsync(&nnz, h->csr_off + n, sizeof(int), cudaMemcpyDeviceToHost, st));
-    EGT_CUDA_TRY(cudaStreamSynchronize(st));
-    h->nnz = nnz;
-    if (h->csr_cap < nnz || !h->csr_col) {
-        if (h->csr_col) EGT_CUDA_TRY(cudaFree(h->csr_col));
+    if (!h->csr_off) EGT_CUDA_TRY(dev_alloc(h, &h->csr_off, sizeof(int) * (n + 1)));
+    const int64_t cap = n * (int64_t)h->k;
+    if (h->csr_cap < cap || !h->csr_col) {
+        dev_free(h, h->csr_col);
         h->csr_col = nullptr;
-        EGT_CUDA_TRY(cudaMalloc(&h->csr_col, sizeof(int) * std::max<int64_t>(nnz, 1)));
-        h->csr_cap = std::max<int64_t>(nnz, 1);
+        EGT_CUDA_TRY(dev_alloc(h, &h->csr_col, sizeof(int) * std::max<int64_t>(cap, 1)));
+        h->csr_cap = std::max<int64_t>(cap, 1);
     }
+    EGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, cub_scan, counts, h->csr_off, (int)(n + 1), st));
     const int k = h->k;
     if (k <= 32) EGT_TRY(launch_compact<1>(h));
     else if (k <= 64) EGT_TRY(launch_compact<2>(h));
     else if (k <= 128) EGT_TRY(launch_compact<4>(h));
     else EGT_TRY(launch_compact<8>(h));
+    h->nnz = -1;  // known on the device; fetched on demand
     h->have_csr = true;
+    h->csr_version++;
+    return EGT_OK;
+}
+
+// Reads the CSR size back from the device (synchronises the stream).
+egt_status csr_nnz(egt_handle* h, int64_t* out) {
+    if (h->nnz < 0) {
+        int v = 0;
+        EGT_CUDA_TRY(cudaMemcpyAsync(&v, h->csr_off + h->n, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        EGT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        h->nnz = v;
+    }
+    *out = h->nnz;
     return EGT_OK;
 }
 
@@ -210,6 +237,7 @@ egt_status run_egt(egt_handle* h, float alpha) {
     else if (k <= 64) s = launch_egt<2>(h, alpha, counts);
     else if (k <= 128) s = launch_egt<4>(h, alpha, counts);
     else s = launch_egt<8>(h, alpha, counts);
+    EGT_CUDA_TRY(cudaEventRecord(h->ev[14], st));
     if (s == EGT_OK) s = build_csr(h, counts);
     EGT_CUDA_TRY(cudaEventRecord(h->ev[5], st));
     cudaFreeAsync(counts, st);

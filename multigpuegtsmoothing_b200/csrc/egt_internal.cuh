@@ -148,7 +148,7 @@ struct egt_handle {
     int* csr_off = nullptr;      // [n+1]
     int* csr_col = nullptr;      // [nnz]
     int64_t csr_cap = 0;
-    int64_t nnz = 0;
+    int64_t nnz = 0;             // -1 while only the device knows it
     bool have_csr = false;
     // mesh
     uint32_t* tris = nullptr;    // [3t] sorted-space triangle corners
@@ -157,6 +157,21 @@ struct egt_handle {
     float* nrm = nullptr;        // [3n] SoA sorted-space normals
     // device counters
     unsigned long long* d_counters = nullptr;  // [kCtrWords] device counters
+    // Taubin working set in Morton order of the level-0 cells
+    int* m_perm = nullptr;       // [n] Morton position -> sorted index
+    int* m_inv = nullptr;        // [n] sorted index -> Morton position
+    float4* m_p = nullptr;       // [n] positions (Morton order)
+    float4* m_pb = nullptr;      // [n] ping-pong
+    int* m_off = nullptr;        // [n+1]
+    int* m_col = nullptr;        // [nnz]
+    int64_t m_cap = 0;
+    // per 256-row tile: distinct neighbour indices (stored at the tile's first
+    // CSR offset) and, per CSR entry, its index into that list
+    int* t_uni = nullptr;        // [nnz]
+    uint16_t* t_loc = nullptr;   // [nnz]
+    int* t_nu = nullptr;         // [tiles] distinct count, -1 = tile not staged
+    uint64_t csr_version = 0;    // bumped whenever the CSR is rebuilt
+    uint64_t m_version = ~0ull;  // CSR version the Morton copy was built from
     // cached Taubin graph (2*iters half-steps) and the parameters it was built for
     cudaGraphExec_t taubin_exec = nullptr;
     int taubin_iters = -1;
@@ -169,12 +184,23 @@ struct egt_handle {
 };
 
 namespace egt {
+// Handle buffers come from the device's stream-ordered memory pool (kept warm
+// with a high release threshold), so creating and destroying providers
+// repeatedly reuses memory instead of returning it to the driver.
+template <typename T>
+inline cudaError_t dev_alloc(egt_handle* h, T** p, size_t bytes) {
+    return cudaMallocAsync(reinterpret_cast<void**>(p), bytes, h->stream);
+}
+inline void dev_free(egt_handle* h, void* p) {
+    if (p) cudaFreeAsync(p, h->stream);
+}
 egt_status scratch_reserve(egt_handle* h, size_t bytes, void** out);
 egt_status build_grid(egt_handle* h, const float* xyz_dev_aos, int levels);
 egt_status run_knn(egt_handle* h, int k);
 egt_status run_mesh_1ring(egt_handle* h, int k);
 egt_status run_egt(egt_handle* h, float alpha);
 egt_status ensure_csr(egt_handle* h);
+egt_status csr_nnz(egt_handle* h, int64_t* out);
 egt_status run_taubin(egt_handle* h, int iters, float lambda, float mu);
 egt_status run_normals(egt_handle* h);
 egt_status run_orient(egt_handle* h);

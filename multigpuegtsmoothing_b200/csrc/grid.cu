@@ -4,7 +4,8 @@
 // getBuckets / InitializeLevel (GridKNNCuda.cu:898-946).
 //
 // Layout produced in HBM (all in cell-sorted order):
-//   p4[n]      float4 (x,y,z,0) normalised positions   -- kernels read these
+//   p4[n]      float4 (x,y,z,c) normalised positions; c = the packed level-0
+//              cell coordinates (bit pattern), read together with the position
 //   x/y/z[n]   SoA mirror                              -- KNNInterface views
 //   cell0[n]   packed level-0 cell coords x|y<<10|z<<20
 //   perm[n]    sorted slot -> original index
@@ -117,11 +118,13 @@ __global__ void k_gather_sorted(const float4* __restrict__ tmp4, const int* __re
     if (s >= n) return;
     const NormParams p = *np;
     float4 v = tmp4[perm[s]];
-    p4[s] = v;
     x[s] = v.x; y[s] = v.y; z[s] = v.z;
     uint32_t xi = cell_coord(v.x, p.a, p.b, 1024), yi = cell_coord(v.y, p.a, p.b, 1024),
              zi = cell_coord(v.z, p.a, p.b, 1024);
-    cell0[s] = xi | (yi << 10) | (zi << 20);
+    const uint32_t packed = xi | (yi << 10) | (zi << 20);
+    cell0[s] = packed;
+    v.w = __uint_as_float(packed);  // the kNN reads a candidate's cell with its position
+    p4[s] = v;
 }
 
 __global__ void k_level_key(const uint32_t* __restrict__ cell0, int64_t n, int L, uint32_t* __restrict__ key,
@@ -177,13 +180,12 @@ __global__ void k_cells(const uint32_t* __restrict__ key, const int* __restrict_
 egt_status scratch_reserve(egt_handle* h, size_t bytes, void** out) {
     if (h->scratch.bytes < bytes) {
         if (h->scratch.ptr) {
-            EGT_CUDA_TRY(cudaStreamSynchronize(h->stream));
-            EGT_CUDA_TRY(cudaFree(h->scratch.ptr));
+            dev_free(h, h->scratch.ptr);  // stream-ordered: pending work keeps it until done
             h->scratch.ptr = nullptr;
             h->scratch.bytes = 0;
         }
         size_t want = bytes + bytes / 4 + 256;
-        EGT_CUDA_TRY(cudaMalloc(&h->scratch.ptr, want));
+        EGT_CUDA_TRY(dev_alloc(h, &h->scratch.ptr, want));
         h->scratch.bytes = want;
     }
     *out = h->scratch.ptr;
@@ -228,7 +230,7 @@ static egt_status build_levels(egt_handle* h, const uint32_t* sorted_key0, int l
             key = sorted_key0;
             lv.order = nullptr;
         } else {
-            if (!lv.order) EGT_CUDA_TRY(cudaMalloc(&lv.order, sizeof(int) * n));
+            if (!lv.order) EGT_CUDA_TRY(dev_alloc(h, &lv.order, sizeof(int) * n));
             k_level_key<<<G, T, 0, st>>>(h->cell0, n, L, keyA, idx);
             EGT_LAUNCH_CHECK();
             size_t tb = cub_sort;
@@ -236,9 +238,9 @@ static egt_status build_levels(egt_handle* h, const uint32_t* sorted_key0, int l
                                                          3 * (10 - L), st));
             key = keyB;
         }
-        if (!lv.cell_start) EGT_CUDA_TRY(cudaMalloc(&lv.cell_start, sizeof(int) * (n + 1)));
-        if (!lv.cell_x) EGT_CUDA_TRY(cudaMalloc(&lv.cell_x, sizeof(int) * n));
-        if (!lv.row_range) EGT_CUDA_TRY(cudaMalloc(&lv.row_range, sizeof(int2) * (size_t)lv.B * lv.B));
+        if (!lv.cell_start) EGT_CUDA_TRY(dev_alloc(h, &lv.cell_start, sizeof(int) * (n + 1)));
+        if (!lv.cell_x) EGT_CUDA_TRY(dev_alloc(h, &lv.cell_x, sizeof(int) * n));
+        if (!lv.row_range) EGT_CUDA_TRY(dev_alloc(h, &lv.row_range, sizeof(int2) * (size_t)lv.B * lv.B));
         EGT_CUDA_TRY(cudaMemsetAsync(lv.row_range, 0, sizeof(int2) * (size_t)lv.B * lv.B, st));
         k_head_flags<<<G, T, 0, st>>>(key, n, flag);
         EGT_LAUNCH_CHECK();

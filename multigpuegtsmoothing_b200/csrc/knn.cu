@@ -5,7 +5,7 @@
 // The reference runs one launch per shell cell (27 launches for the own cell
 // and ring 1, 26 per further level), each followed by a device sync, a host
 // reduction and a compaction of the still-searching queries.  Here one warp
-// runs one query through the whole sequence in a single launch:
+// runs a query through the whole sequence in a single launch:
 //
 //   own level-0 cell; decide; ring 1 at level 0; decide; ring 1 at level 1; ...
 //   ring 1 at level 7 (B = 8); a query still searching after that is invalid.
@@ -17,6 +17,13 @@
 // bit-identical to the reference's.  The 26 shell cells of a level are
 // resolved in parallel (one per lane) and their points are streamed as one
 // flattened candidate sequence, 32 candidates per step.
+//
+// Re-visits are skipped: the cells visited up to level L-1 form the 3x3x3
+// block of level L-1 around the query, and the level-L ring covers it again.
+// A point of that block was already offered to the list: it is either in the
+// list (the dedup rule rejects it) or farther than the k-th distance of that
+// time, which never grows (the admission rule rejects it), so offering it again
+// cannot change the list.
 #include "egt_internal.cuh"
 #include "knn_common.cuh"
 
@@ -25,7 +32,6 @@ namespace {
 
 struct KnnArgs {
     const float4* __restrict__ p4;
-    const uint32_t* __restrict__ cell0;
     const NormParams* __restrict__ np;
     LevelDev lv[kMaxLevels];
     int n, k, max_pts;
@@ -68,12 +74,13 @@ __device__ __forceinline__ bool decide(const NormParams& np, int L, int o, int c
 // Streams the points of `m` cells (cell l held by lane l as [cs, ce), ce < 0 =
 // empty) through the list, in cell order.  Sets `invalid` when a visited cell
 // holds >= max_pts points (GridKNNCuda.cu:672, 685): the cells before it are
-// still processed, the rest are not.
+// still processed, the rest are not.  skipL >= 0: skip points whose level-skipL
+// cell lies in the 3x3x3 block around the query's (already visited).
 template <int S>
 __device__ __forceinline__ void stream_cells(WarpList<S>& L, bool& invalid, int m, int cs, int ce,
                                              const int* __restrict__ order, const float4* __restrict__ p4,
                                              int q, float4 pq, float thres, int max_pts, int lane,
-                                             int* s_pref, int* s_start) {
+                                             int skipL, uint32_t qc0, int* s_pref, int* s_start) {
     const bool exists = lane < m && ce >= 0;
     const bool big = exists && (ce - cs) >= max_pts;
     const unsigned bigmask = __ballot_sync(0xffffffffu, big);
@@ -86,9 +93,12 @@ __device__ __forceinline__ void stream_cells(WarpList<S>& L, bool& invalid, int 
         if (lane >= o) incl += v;
     }
     const int total = __shfl_sync(0xffffffffu, incl, 31);
+    __syncwarp();
     s_pref[lane] = incl;
     s_start[lane] = cs;
     __syncwarp();
+    const int qx = (int)((qc0 & 1023u) >> max(skipL, 0)), qy = (int)(((qc0 >> 10) & 1023u) >> max(skipL, 0)),
+              qz = (int)(((qc0 >> 20) & 1023u) >> max(skipL, 0));
     for (int base = 0; base < total; base += 32) {
         const int j = base + lane;
         float d = 1e30f;
@@ -106,8 +116,17 @@ __device__ __forceinline__ void stream_cells(WarpList<S>& L, bool& invalid, int 
             p = order ? order[pos] : pos;
             if (p != q) {
                 const float4 v = p4[p];
-                d = fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z);
-                ok = d <= thres;
+                bool fresh = true;
+                if (skipL >= 0) {
+                    const uint32_t c = __float_as_uint(v.w);
+                    const int px = (int)((c & 1023u) >> skipL), py = (int)(((c >> 10) & 1023u) >> skipL),
+                              pz = (int)(((c >> 20) & 1023u) >> skipL);
+                    fresh = abs(px - qx) > 1 || abs(py - qy) > 1 || abs(pz - qz) > 1;
+                }
+                if (fresh) {
+                    d = fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z);
+                    ok = d <= thres;
+                }
             }
         }
         unsigned mask = __ballot_sync(0xffffffffu, ok && d < L.kth);
@@ -119,8 +138,39 @@ __device__ __forceinline__ void stream_cells(WarpList<S>& L, bool& invalid, int 
             L.insert(dd, pp, lane);
         }
     }
-    __syncwarp();
     if (bigmask) invalid = true;
+}
+
+// The whole reference search for query q.  Returns the level reached
+// (kMaxLevels when the query ran out of levels).
+template <int S>
+__device__ int search(const KnnArgs& a, const NormParams& np, int q, float4 pq, WarpList<S>& L,
+                      bool& invalid, int lane, int* s_pref, int* s_start) {
+    const uint32_t c0 = __float_as_uint(pq.w);
+    const int cx0 = c0 & 1023, cy0 = (c0 >> 10) & 1023, cz0 = (c0 >> 20) & 1023;
+    L.init(a.k);
+    invalid = false;
+    // offset 0 at level 0: the query's own cell (always occupied)
+    int2 own = lane == 0 ? find_cell(a.lv[0], cx0, cy0, cz0) : make_int2(-1, -1);
+    stream_cells<S>(L, invalid, 1, own.x, own.y, nullptr, a.p4, q, pq, np.thres, a.max_pts, lane, -1, c0, s_pref,
+                    s_start);
+    bool cont = decide(np, 0, 0, L.counter, L.k, L.kth, invalid, pq, cx0, cy0, cz0);
+    int reached = 0;
+    for (int lvl = 0; cont; lvl++) {
+        reached = lvl;
+        const LevelDev& LV = a.lv[lvl];
+        int2 cell = make_int2(-1, -1);
+        if (lane < 26)
+            cell = find_cell(LV, (cx0 >> lvl) + kShell[lane][0], (cy0 >> lvl) + kShell[lane][1],
+                             (cz0 >> lvl) + kShell[lane][2]);
+        stream_cells<S>(L, invalid, 26, cell.x, cell.y, LV.order, a.p4, q, pq, np.thres, a.max_pts, lane, lvl - 1,
+                        c0, s_pref, s_start);
+        cont = decide(np, lvl, 1, L.counter, L.k, L.kth, invalid, pq, cx0, cy0, cz0);
+        if (lvl == kMaxLevels - 1) break;
+    }
+    // still searching after the B = 8 ring: invalid (GridKNNCuda.cu:2572-2586)
+    if (cont) { invalid = true; reached = kMaxLevels; }
+    return reached;
 }
 
 template <int S>
@@ -132,32 +182,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_knn_plain(KnnArgs a) {
     if (q >= a.n) return;
     const NormParams np = *a.np;
     const float4 pq = a.p4[q];
-    const uint32_t c0 = a.cell0[q];
-    const int cx0 = c0 & 1023, cy0 = (c0 >> 10) & 1023, cz0 = (c0 >> 20) & 1023;
     WarpList<S> L;
-    L.init(a.k);
-    bool invalid = false;
-
-    // offset 0 at level 0: the query's own cell (always occupied)
-    int2 own = lane == 0 ? find_cell(a.lv[0], cx0, cy0, cz0) : make_int2(-1, -1);
-    stream_cells<S>(L, invalid, 1, own.x, own.y, nullptr, a.p4, q, pq, np.thres, a.max_pts, lane,
-                    s_pref[w], s_start[w]);
-    bool cont = decide(np, 0, 0, L.counter, L.k, L.kth, invalid, pq, cx0, cy0, cz0);
-    int reached = 0;
-    for (int lvl = 0; cont; lvl++) {
-        reached = lvl;
-        const LevelDev& LV = a.lv[lvl];
-        int2 cell = make_int2(-1, -1);
-        if (lane < 26)
-            cell = find_cell(LV, (cx0 >> lvl) + kShell[lane][0], (cy0 >> lvl) + kShell[lane][1],
-                             (cz0 >> lvl) + kShell[lane][2]);
-        stream_cells<S>(L, invalid, 26, cell.x, cell.y, LV.order, a.p4, q, pq, np.thres, a.max_pts, lane,
-                        s_pref[w], s_start[w]);
-        cont = decide(np, lvl, 1, L.counter, L.k, L.kth, invalid, pq, cx0, cy0, cz0);
-        if (lvl == kMaxLevels - 1) break;
-    }
-    // still searching after the B = 8 ring: invalid (GridKNNCuda.cu:2572-2586)
-    if (cont) { invalid = true; reached = kMaxLevels; }
+    bool invalid;
+    const int reached = search<S>(a, np, q, pq, L, invalid, lane, s_pref[w], s_start[w]);
 #pragma unroll
     for (int s = 0; s < S; s++) {
         const int t = lane + 32 * s;
@@ -187,18 +214,17 @@ egt_status run_knn(egt_handle* h, int k) {
     cudaStream_t st = h->stream;
     const int64_t n = h->n;
     if (h->k != k || !h->lists) {
-        if (h->lists) EGT_CUDA_TRY(cudaFree(h->lists));
+        if (h->lists) dev_free(h, h->lists);
         h->lists = nullptr;
-        EGT_CUDA_TRY(cudaMalloc(&h->lists, sizeof(int) * (size_t)n * k));
+        EGT_CUDA_TRY(dev_alloc(h, &h->lists, sizeof(int) * (size_t)n * k));
         h->k = k;
     }
-    if (!h->kth) EGT_CUDA_TRY(cudaMalloc(&h->kth, sizeof(float) * n));
-    if (!h->qlevel) EGT_CUDA_TRY(cudaMalloc(&h->qlevel, n));
+    if (!h->kth) EGT_CUDA_TRY(dev_alloc(h, &h->kth, sizeof(float) * n));
+    if (!h->qlevel) EGT_CUDA_TRY(dev_alloc(h, &h->qlevel, n));
     h->have_csr = false;
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
     KnnArgs a;
     a.p4 = h->p4;
-    a.cell0 = h->cell0;
     a.np = h->d_norm;
     for (int L = 0; L < kMaxLevels; L++) a.lv[L] = h->lv[L];
     a.n = (int)n;

@@ -25,6 +25,7 @@ struct WarpList {
     int counter;  // number of filled slots (uniform)
     float kth;    // value of slot k-1 (uniform): 1e10 until the list is full
     int k;
+    bool tie;     // an insertion met an equal distance already in the list
 
     __device__ __forceinline__ void init(int k_) {
 #pragma unroll
@@ -32,6 +33,7 @@ struct WarpList {
         counter = 0;
         kth = 1e10f;
         k = k_;
+        tie = false;
     }
 
     __device__ __forceinline__ float fetch_dist(int t) const {
@@ -60,6 +62,7 @@ struct WarpList {
         if (!__any_sync(0xffffffffu, eq)) {
             pos = (int)lt;  // no equal element: FindPosition returns the insertion point
         } else {
+            tie = true;
             int low = 0, high = counter - 1;
             pos = -1;
             while (low <= high) {  // at most log2(k)+1 iterations

@@ -116,9 +116,9 @@ egt_status run_mesh_1ring(egt_handle* h, int k) {
     cudaStream_t st = h->stream;
     const int64_t n = h->n, t = h->t, m = 3 * t;
     if (h->k != k || !h->lists) {
-        if (h->lists) EGT_CUDA_TRY(cudaFree(h->lists));
+        if (h->lists) dev_free(h, h->lists);
         h->lists = nullptr;
-        EGT_CUDA_TRY(cudaMalloc(&h->lists, sizeof(int) * (size_t)n * k));
+        EGT_CUDA_TRY(dev_alloc(h, &h->lists, sizeof(int) * (size_t)n * k));
         h->k = k;
     }
     h->have_csr = false;

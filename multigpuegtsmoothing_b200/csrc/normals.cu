@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(128) k_normals(const float4* __restrict__ p4, 
 egt_status run_normals(egt_handle* h) {
     EGT_TRY(ensure_csr(h));
     const int n = (int)h->n;
-    if (!h->nrm) EGT_CUDA_TRY(cudaMalloc(&h->nrm, sizeof(float) * 3 * (size_t)n));
+    if (!h->nrm) EGT_CUDA_TRY(dev_alloc(h, &h->nrm, sizeof(float) * 3 * (size_t)n));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrNormFallback, 0, sizeof(unsigned long long), h->stream));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[8], h->stream));
     k_normals<<<(unsigned)((n + 127) / 128), 128, 0, h->stream>>>(h->p4, h->csr_off, h->csr_col, n,

@@ -160,7 +160,8 @@ __global__ void k_apply(int n, int bits, const int* __restrict__ comp, const sig
 egt_status run_orient(egt_handle* h) {
     cudaStream_t st = h->stream;
     const int n = (int)h->n;
-    const int64_t nnz = h->nnz;
+    int64_t nnz = 0;
+    EGT_TRY(csr_nnz(h, &nnz));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[10], st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrMsf, 0, 2 * sizeof(unsigned long long), st));
     if (nnz == 0 || n < 2) {

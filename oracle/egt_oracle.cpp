@@ -649,7 +649,7 @@ void orc_taubin_f32(float* pos, int n, int k, const int* lists, int iters, float
                 int m = row[j];
                 if (m == -1) continue;
                 float x2 = in[m], y2 = in[n + m], z2 = in[2 * (size_t)n + m];
-                float w = std::exp(-dist3(x1, y1, z1, x2, y2, z2));
+                float w = std::exp(-dist3_taubin(x1, y1, z1, x2, y2, z2));
                 cx = acc(cx, w, x2 - x1); cy = acc(cy, w, y2 - y1); cz = acc(cz, w, z2 - z1);
                 sum += w;
             }

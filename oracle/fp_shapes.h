@@ -6,7 +6,9 @@
 // result, and the last bit decides ties and near-ties in the kNN ordering.
 // The shapes below were identified black-box (a probe kernel compiled with the
 // same flags, evaluated on random inputs and compared against each candidate
-// written with an explicit fma); the CUDA kernels use the same shapes through
+// written with an explicit fma, and -- where the compiler's choice depends on
+// the surrounding code -- candidates compared against the reference's own
+// outputs); the CUDA kernels use the same shapes through
 // __fmaf_rn/__fmul_rn/__fadd_rn so that they, this oracle and the reference
 // round identically.  The CPU side must be compiled with -ffp-contract=off.
 #pragma once
@@ -18,6 +20,14 @@ namespace fpshape {
 inline float dist3(float ax, float ay, float az, float bx, float by, float bz) {
     float dx = ax - bx, dy = ay - by, dz = az - bz;
     return std::fmaf(dz, dz, std::fmaf(dx, dx, dy * dy));
+}
+// The same expression as contracted inside taubin_step_GKNN (EGT_CUDA.cu:258):
+// fma(dz,dz, fma(dy,dy, dx*dx)).  The compiler pairs the operands differently
+// there than in the kNN distance; identified against the reference's own
+// smoothed positions.
+inline float dist3_taubin(float ax, float ay, float az, float bx, float by, float bz) {
+    float dx = ax - bx, dy = ay - by, dz = az - bz;
+    return std::fmaf(dz, dz, std::fmaf(dy, dy, dx * dx));
 }
 // x*x + y*y + z*z  (EGT_CUDA.cu:53-56, 147)
 inline float sq3(float x, float y, float z) { return std::fmaf(z, z, std::fmaf(x, x, y * y)); }

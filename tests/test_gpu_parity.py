@@ -35,8 +35,9 @@ def test_knn_egt_taubin_output_match_reference(capi, oracle, name):
     capi.EGT_CUDA(g).PerformSmoothing(m["iters"], 0.63, -0.64, m["alpha"])
     assert np.array_equal(g.sorted_lists(), d["ref_knn_egt"])
     pos = g.sorted_positions()
-    # smoothed positions: within 1e-6 of the bbox diagonal of the reference's
-    # FP32 result and of the FP64 oracle (original units)
+    # smoothed positions: the reference's FP32 result bit for bit, and within
+    # 1e-6 of the bbox diagonal of the FP64 oracle (original units)
+    assert np.array_equal(pos, d["ref_pos_out"])
     scale = float(d["ref_extents"][1]) - float(d["ref_extents"][0])
     tol = 1e-6 * bbox_diag(d["in_xyz"])
     assert np.abs(pos - d["ref_pos_out"]).max() * scale <= tol
@@ -58,6 +59,7 @@ def test_mesh_matches_reference(capi, name):
     assert np.array_equal(got, d["ref_knn_raw"])
     capi.EGT_CUDA(g).PerformSmoothing(m["iters"], 0.63, -0.64, m["alpha"])
     assert np.array_equal(g.sorted_lists(), d["ref_knn_egt"])
+    assert np.array_equal(g.sorted_positions(), d["ref_pos_out"])
     scale = float(d["ref_extents"][1]) - float(d["ref_extents"][0])
     assert np.abs(g.sorted_positions() - d["ref_pos_out"]).max() * scale <= 1e-6 * bbox_diag(d["in_xyz"])
 
@@ -82,8 +84,9 @@ def test_full_size_configs_match_reference(capi, oracle, name):
     p0 = oracle.knn(xyz, m["k"]) if tris is None else oracle.mesh_1ring(xyz, tris, m["k"])
     scale = float(p0["ext"][1]) - float(p0["ext"][0])
     tol = 1e-6 * bbox_diag(xyz)
-    # FP32 smoothing against the reference's FP32 result and the FP64 oracle
-    assert np.abs(pos[:, rows] - d["ref_pos_out_cols"]).max() * scale <= tol
+    # FP32 smoothing: the reference's result bit for bit (sampled rows), and
+    # within 1e-6 of the bbox diagonal of the FP64 oracle
+    assert np.array_equal(pos[:, rows], d["ref_pos_out_cols"])
     p64 = oracle.taubin_f64(p0["pos"], lists, m["iters"])
     assert np.abs(pos - p64).max() * scale <= tol
 
