@@ -35,6 +35,16 @@ typedef int egt_status;
 #define EGT_ERR_NOMEM         -6  /* device allocation failed */
 
 typedef struct egt_handle egt_handle;
+typedef struct egt_proposal egt_proposal;
+
+/* Learned search proposal network (no reference counterpart): 8 features ->
+ * 32 -> 32 -> 16 classes, binary16 parameters. */
+#define EGT_PROPOSAL_FEATURES 8
+#define EGT_PROPOSAL_CLASSES 16
+#define EGT_PROPOSAL_PARAMS 1872
+
+#define EGT_KNN_PLAIN 0
+#define EGT_KNN_LEARNED 1
 
 /* Tunables.  Defaults reproduce the reference CLI (main.cpp:108-116). */
 typedef struct egt_config {
@@ -43,7 +53,8 @@ typedef struct egt_config {
     int bucket_count;        /* level-0 buckets per axis (1024) */
     float threshold;         /* GRIDCUDAKNNSELF_COMPACT thres before scaling (1e8) */
     int max_points_in_cell;  /* MAX_PNTS_IN_CUBE (100000): larger cells invalidate a query */
-    int knn_mode;            /* 0 = plain hierarchical ring search, 1 = learned proposal */
+    int knn_mode;            /* EGT_KNN_PLAIN, or EGT_KNN_LEARNED: egt_knn uses the proposal
+                                attached with egt_attach_proposal */
     int warps_per_block;     /* kNN/EGT launch shape (0 = autotuned default) */
     float normals_gap_tol;   /* FP64 eigensolve when (l1-l0) < tol*l2 (0.1; 0 = FP32 only) */
 } egt_config;
@@ -72,6 +83,11 @@ typedef struct egt_timings {
     int64_t msf_edges;       /* edges of the orientation spanning forest */
     int components;          /* orientation components (trees with >= 1 edge) */
     float egt_kernel_ms;     /* the EGT filter kernel alone (egt_ms also packs the CSR) */
+    float propose_ms;        /* learned kNN: features + proposal network (inside knn_ms) */
+    int64_t box_queries;     /* learned kNN: queries that ran a proposed box search */
+    int64_t certified_queries; /* learned kNN: box results certified (the rest ran the plain search) */
+    int64_t exact_reruns;    /* kNN queries whose kept distances tied and that were searched again
+                                with the reference's one-at-a-time insertion rule */
 } egt_timings;
 
 void egt_default_config(egt_config* cfg);
@@ -144,6 +160,54 @@ egt_status egt_get_csr(egt_handle* h, const int** offsets, const int** cols, int
  * serialised by the caller. */
 egt_status egt_taubin_noalloc(const float* pos_in, float* pos_out, const int* csr_off, const int* csr_col,
                               int64_t n, int iters, float lambda, float mu, void* stream);
+
+/* ---- Learned search proposal (no reference counterpart) ------------------
+ * A small MLP predicts, per query, a box of grid cells around it (16 classes:
+ * 15 boxes of growing size and "plain search") from 8 cell-occupancy
+ * features.  The kNN kernel searches the proposed box and keeps its result
+ * only when it is certified equal to the plain search's (k-th distance ball
+ * inside the box, distinct distances, the plain stop level replayed, no
+ * oversized cell); otherwise the plain search runs.  Lists are therefore
+ * bit-identical to egt_knn's plain mode whatever the network predicts.
+ * Training runs on the device (hand-written forward/backward/Adam kernels,
+ * binary16 parameters with FP32 accumulation and FP32 master copies) on labels
+ * produced by the plain kNN: the smallest certifying box of each query. */
+egt_status egt_proposal_create(int device, int k, uint64_t seed, egt_proposal** out);
+void egt_proposal_destroy(egt_proposal* p);
+/* Appends the features and labels of every `stride`-th query of h to the
+ * training set.  h must hold a plain (or learned) kNN with the proposal's k. */
+egt_status egt_proposal_collect(egt_proposal* p, egt_handle* h, int stride);
+/* Number of training samples collected so far. */
+int64_t egt_proposal_samples(const egt_proposal* p);
+/* `steps` Adam steps on mini-batches of `batch` samples drawn with
+ * replacement; loss_out (optional, host [steps]) receives each step's mean
+ * cross-entropy. */
+egt_status egt_proposal_train(egt_proposal* p, int steps, int batch, float lr, float* loss_out);
+/* One forward/backward pass over m given samples (host feats [m*8], labels
+ * [m]) with the current parameters: grads (host [EGT_PROPOSAL_PARAMS]) of the
+ * mean cross-entropy, loss (host, optional).  For gradient checks. */
+egt_status egt_proposal_gradients(egt_proposal* p, const float* feats, const uint8_t* labels, int m, float* grads,
+                                  float* loss);
+/* Parameters as binary16 bit patterns, layout W1[32][8] b1 W2[32][32] b2 W3[16][32] b3. */
+egt_status egt_proposal_get_params(const egt_proposal* p, uint16_t* params);
+egt_status egt_proposal_set_params(egt_proposal* p, const uint16_t* params);
+/* Class choice: the smallest class whose predicted cumulative probability
+ * reaches tau (default 0.85). */
+egt_status egt_proposal_set_tau(egt_proposal* p, float tau);
+float egt_proposal_get_tau(const egt_proposal* p);
+/* Autotuner: times the learned kNN on h (which must have been searched with
+ * the proposal's k) for each of the ntau thresholds and keeps the fastest;
+ * ms_out (optional, host [ntau]) receives the times. */
+egt_status egt_proposal_tune(egt_proposal* p, egt_handle* h, const float* taus, int ntau, float* ms_out);
+/* Features [n*8], labels [n] (from the handle's last kNN) and proposed
+ * classes [n] of every query, sorted space, to host (any may be NULL). */
+egt_status egt_proposal_inspect(const egt_proposal* p, egt_handle* h, float* feats, uint8_t* labels,
+                                uint8_t* classes);
+/* Learned-mode kNN: same outputs as egt_knn (bit-identical lists). */
+egt_status egt_knn_learned(egt_handle* h, int k, const egt_proposal* p, void* stream);
+/* Makes egt_knn use p when cfg.knn_mode == EGT_KNN_LEARNED (NULL detaches).
+ * The proposal must outlive the attachment. */
+egt_status egt_attach_proposal(egt_handle* h, const egt_proposal* p);
 
 /* Copies bytes from device memory (e.g. a pointer from egt_get_views) to host
  * memory after synchronising the handle's stream.  No reference counterpart:

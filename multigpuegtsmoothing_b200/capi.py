@@ -55,7 +55,8 @@ class Timings(C.Structure):
                 ("normals_ms", C.c_float), ("orient_ms", C.c_float), ("output_ms", C.c_float),
                 ("levels_used", C.c_int), ("invalid_queries", C.c_int64), ("csr_nnz", C.c_int64),
                 ("normals_fp64", C.c_int64), ("msf_edges", C.c_int64), ("components", C.c_int),
-                ("egt_kernel_ms", C.c_float)]
+                ("egt_kernel_ms", C.c_float), ("propose_ms", C.c_float), ("box_queries", C.c_int64),
+                ("certified_queries", C.c_int64), ("exact_reruns", C.c_int64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -97,6 +98,20 @@ def lib() -> C.CDLL:
             "egt_kernel_launches": (i64, []),
             "egt_taubin_noalloc": (i32, [vp, vp, vp, vp, i64, i32, f32, f32, vp]),
             "egt_destroy": (None, [vp]),
+            "egt_proposal_create": (i32, [i32, i32, C.c_uint64, hp]),
+            "egt_proposal_destroy": (None, [vp]),
+            "egt_proposal_collect": (i32, [vp, vp, i32]),
+            "egt_proposal_samples": (i64, [vp]),
+            "egt_proposal_train": (i32, [vp, i32, i32, f32, vp]),
+            "egt_proposal_gradients": (i32, [vp, vp, vp, i32, vp, vp]),
+            "egt_proposal_get_params": (i32, [vp, vp]),
+            "egt_proposal_set_params": (i32, [vp, vp]),
+            "egt_proposal_set_tau": (i32, [vp, f32]),
+            "egt_proposal_get_tau": (f32, [vp]),
+            "egt_proposal_tune": (i32, [vp, vp, vp, i32, vp]),
+            "egt_proposal_inspect": (i32, [vp, vp, vp, vp, vp]),
+            "egt_knn_learned": (i32, [vp, i32, vp, vp]),
+            "egt_attach_proposal": (i32, [vp, vp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -111,7 +126,7 @@ def exported_symbols():
     import re
     hdr = os.path.join(os.path.dirname(HERE), "include", "egt_b200.h")
     txt = open(hdr).read()
-    return sorted(set(re.findall(r"^\s*(?:egt_status|void|int64_t|const char\*)\s+(egt_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:egt_status|void|int64_t|int|float|const char\*)\s+(egt_\w+)\s*\(", txt, re.M)))
 
 
 def _check(st: int):
@@ -263,6 +278,11 @@ class GridStructure(_Handle):
             raise EgtError(-2, "thres is fixed at creation (config.threshold)")
         _check(lib().egt_knn(self.handle, int(k), self.stream))
 
+    def GRIDCUDAKNNSELF_LEARNED(self, k: int, proposal: "SearchProposal"):
+        """The same search driven by a learned proposal: lists bit-identical to
+        GRIDCUDAKNNSELF_COMPACT (no reference counterpart)."""
+        _check(lib().egt_knn_learned(self.handle, int(k), proposal.handle, self.stream))
+
 
 class GridMeshCuda(_Handle):
     """Mesh provider: GridMeshCuda(mesh, 1, eps, 1024) (GridMeshCuda1.cu:247-414)."""
@@ -327,3 +347,96 @@ def getOutputPoints(provider: _Handle) -> Tuple[np.ndarray, np.ndarray, np.ndarr
     x, y, z = (np.empty(n, np.float32) for _ in range(3))
     _check(lib().egt_output(provider.handle, _ptr(x), _ptr(y), _ptr(z), provider.stream))
     return x, y, z
+
+
+PROPOSAL_PARAMS = 1872
+PROPOSAL_CLASSES = 16
+PROPOSAL_FEATURES = 8
+
+
+class SearchProposal:
+    """Learned search proposal (egt_proposal_*; no reference counterpart).
+
+    An MLP 8 -> 32 -> 32 -> 16 with binary16 parameters proposes, per query, a
+    box of grid cells for the kNN search; the search certifies the box result
+    or falls back to the plain search, so lists never change.  Training data
+    comes from providers that ran the plain search (collect), training runs on
+    the GPU (train), and tune() picks the class threshold by timing.
+    """
+
+    def __init__(self, k: int, seed: int = 0, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().egt_proposal_create(int(device), int(k), C.c_uint64(seed), C.byref(h)))
+        self._h = h
+        self.k = int(k)
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise EgtError(-5, "proposal destroyed")
+        return self._h
+
+    def close(self):
+        if self._h is not None:
+            lib().egt_proposal_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def collect(self, provider: _Handle, stride: int = 1):
+        _check(lib().egt_proposal_collect(self.handle, provider.handle, int(stride)))
+
+    @property
+    def samples(self) -> int:
+        return int(lib().egt_proposal_samples(self.handle))
+
+    def train(self, steps: int, batch: int = 4096, lr: float = 3e-3) -> np.ndarray:
+        loss = np.zeros(max(int(steps), 1), np.float32)
+        _check(lib().egt_proposal_train(self.handle, int(steps), int(batch), float(lr), _ptr(loss)))
+        return loss[:int(steps)]
+
+    def gradients(self, feats: np.ndarray, labels: np.ndarray) -> Tuple[np.ndarray, float]:
+        feats = np.ascontiguousarray(feats, dtype=np.float32).reshape(-1, PROPOSAL_FEATURES)
+        labels = np.ascontiguousarray(labels, dtype=np.uint8).reshape(-1)
+        g = np.zeros(PROPOSAL_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        _check(lib().egt_proposal_gradients(self.handle, _ptr(feats), _ptr(labels), feats.shape[0], _ptr(g),
+                                            _ptr(loss)))
+        return g, float(loss[0])
+
+    def params(self) -> np.ndarray:
+        """binary16 parameters (np.float16, layout W1[32][8] b1 W2[32][32] b2 W3[16][32] b3)."""
+        out = np.zeros(PROPOSAL_PARAMS, np.float16)
+        _check(lib().egt_proposal_get_params(self.handle, _ptr(out)))
+        return out
+
+    def set_params(self, params: np.ndarray):
+        params = np.ascontiguousarray(params, dtype=np.float16)
+        _check(lib().egt_proposal_set_params(self.handle, _ptr(params)))
+
+    @property
+    def tau(self) -> float:
+        return float(lib().egt_proposal_get_tau(self.handle))
+
+    @tau.setter
+    def tau(self, v: float):
+        _check(lib().egt_proposal_set_tau(self.handle, float(v)))
+
+    def tune(self, provider: _Handle, taus=(0.6, 0.75, 0.85, 0.92, 0.97)) -> dict:
+        t = np.ascontiguousarray(taus, dtype=np.float32)
+        ms = np.zeros(len(t), np.float32)
+        _check(lib().egt_proposal_tune(self.handle, provider.handle, _ptr(t), len(t), _ptr(ms)))
+        return dict(zip([float(x) for x in t], [float(x) for x in ms]))
+
+    def inspect(self, provider: _Handle, feats=True, labels=True, classes=True):
+        n = provider.pointsRefCount()
+        f = np.zeros((n, PROPOSAL_FEATURES), np.float32) if feats else None
+        l = np.zeros(n, np.uint8) if labels else None
+        c = np.zeros(n, np.uint8) if classes else None
+        _check(lib().egt_proposal_inspect(self.handle, provider.handle, None if f is None else _ptr(f),
+                                          None if l is None else _ptr(l), None if c is None else _ptr(c)))
+        return f, l, c

@@ -51,7 +51,7 @@ void free_handle(egt_handle* h) {
     for (int L = 0; L < kMaxLevels; L++) {
         F(h->lv[L].order); F(h->lv[L].cell_start); F(h->lv[L].cell_x); F(h->lv[L].row_range);
     }
-    F(h->lists); F(h->kth); F(h->qlevel); F(h->csr_off); F(h->csr_col); F(h->tris); F(h->nrm);
+    F(h->lists); F(h->kth); F(h->qlevel); F(h->pclass); F(h->csr_off); F(h->csr_col); F(h->tris); F(h->nrm);
     F(h->d_counters); F(h->scratch.ptr);
     if (h->taubin_exec) cudaGraphExecDestroy(h->taubin_exec);
     F(h->m_perm); F(h->m_inv); F(h->m_p); F(h->m_pb); F(h->m_off); F(h->m_col);
@@ -194,7 +194,32 @@ egt_status egt_knn(egt_handle* h, int k, void* stream) {
     if ((int64_t)k * h->n > (int64_t)0x7fffffff) { set_error("egt_knn: n*k exceeds 2^31-1"); return EGT_ERR_ARG; }
     EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
     bind_stream(h, stream);
+    if (h->cfg.knn_mode == EGT_KNN_LEARNED) {
+        if (!h->proposal) { set_error("egt_knn: learned mode needs egt_attach_proposal"); return EGT_ERR_STATE; }
+        return egt_knn_learned(h, k, h->proposal, stream);
+    }
+    h->last_knn_learned = false;
     return run_knn(h, k);
+}
+
+egt_status egt_knn_learned(egt_handle* h, int k, const egt_proposal* p, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (!p) { set_error("egt_knn_learned: null proposal"); return EGT_ERR_ARG; }
+    if (h->is_mesh) { set_error("egt_knn_learned: point-cloud handles only"); return EGT_ERR_STATE; }
+    if ((int64_t)k * h->n > (int64_t)0x7fffffff) { set_error("egt_knn_learned: n*k exceeds 2^31-1"); return EGT_ERR_ARG; }
+    if (proposal_k(p) != k) { set_error("egt_knn_learned: k differs from the proposal's k"); return EGT_ERR_ARG; }
+    if (proposal_device(p) != h->cfg.device) { set_error("egt_knn_learned: proposal on another device"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    h->last_knn_learned = true;
+    return run_knn_learned(h, k, p);
+}
+
+egt_status egt_attach_proposal(egt_handle* h, const egt_proposal* p) {
+    EGT_TRY(check_handle(h));
+    if (p && proposal_device(p) != h->cfg.device) { set_error("egt_attach_proposal: proposal on another device"); return EGT_ERR_ARG; }
+    h->proposal = p;
+    return EGT_OK;
 }
 
 egt_status egt_mesh_1ring(egt_handle* h, int k, void* stream) {
@@ -342,6 +367,16 @@ egt_status egt_get_timings(egt_handle* h, egt_timings* t) {
     h->tm.normals_fp64 = (int64_t)ctr[kCtrNormFallback];
     h->tm.msf_edges = (int64_t)ctr[kCtrMsf];
     h->tm.components = (int)ctr[kCtrComps];
+    h->tm.exact_reruns = (int64_t)ctr[kCtrExactRerun];
+    if (h->last_knn_learned) {
+        h->tm.propose_ms = elapsed_ms(h->ev[2], h->ev[15]);
+        h->tm.box_queries = (int64_t)ctr[kCtrBoxTried];
+        h->tm.certified_queries = (int64_t)ctr[kCtrCertified];
+    } else {
+        h->tm.propose_ms = 0.0f;
+        h->tm.box_queries = 0;
+        h->tm.certified_queries = 0;
+    }
     *t = h->tm;
     return EGT_OK;
 }

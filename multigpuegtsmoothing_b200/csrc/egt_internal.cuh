@@ -104,6 +104,11 @@ constexpr int kCtrFlag = 27;      // generic loop flag
 constexpr int kCtrNormFallback = 28;  // normals re-solved in FP64
 constexpr int kCtrMsf = 29;       // spanning-forest edges
 constexpr int kCtrComps = 30;     // orientation components
+constexpr int kCtrMaxPop = 32;    // [32..39] largest cell population per level
+constexpr int kCtrBoxTried = 40;  // learned kNN: queries that ran a box search
+constexpr int kCtrCertified = 41; // learned kNN: certified box results
+constexpr int kCtrExactRerun = 42;  // kNN queries re-searched with the exact insertion rule (ties)
+constexpr int kCtrWork = 43;        // work queue of the persistent kNN kernels (reset with 42)
 
 // One level of the cell hierarchy.  Cells are sorted by key
 // x + y*B + z*B^2; a row is the set of occupied cells sharing (y, z).
@@ -145,6 +150,11 @@ struct egt_handle {
     int* lists = nullptr;        // [n*k] sorted-space lists
     float* kth = nullptr;        // [n] k-th distance per query (diagnostics / learned labels)
     uint8_t* qlevel = nullptr;   // [n] level at which each query stopped
+    // learned search proposal
+    uint8_t* pclass = nullptr;   // [n] proposed class per query
+    bool maxpop_valid = false;   // counters[kCtrMaxPop..] match the current grid
+    const egt_proposal* proposal = nullptr;  // attached for knn_mode == EGT_KNN_LEARNED
+    bool last_knn_learned = false;
     int* csr_off = nullptr;      // [n+1]
     int* csr_col = nullptr;      // [nnz]
     int64_t csr_cap = 0;
@@ -197,6 +207,9 @@ inline void dev_free(egt_handle* h, void* p) {
 egt_status scratch_reserve(egt_handle* h, size_t bytes, void** out);
 egt_status build_grid(egt_handle* h, const float* xyz_dev_aos, int levels);
 egt_status run_knn(egt_handle* h, int k);
+egt_status run_knn_learned(egt_handle* h, int k, const egt_proposal* p);
+int proposal_k(const egt_proposal* p);
+int proposal_device(const egt_proposal* p);
 egt_status run_mesh_1ring(egt_handle* h, int k);
 egt_status run_egt(egt_handle* h, float alpha);
 egt_status ensure_csr(egt_handle* h);

@@ -259,6 +259,7 @@ static egt_status build_levels(egt_handle* h, const uint32_t* sorted_key0, int l
 egt_status build_grid(egt_handle* h, const float* xyz, int levels) {
     const int64_t n = h->n;
     cudaStream_t st = h->stream;
+    h->maxpop_valid = false;
     const int T = 256;
     const unsigned G = (unsigned)((n + T - 1) / T);
     EGT_CUDA_TRY(cudaEventRecord(h->ev[0], st));

@@ -99,6 +99,126 @@ struct WarpList {
     }
 };
 
+// Sorted insertion without the reference's dedup and tie rules, for candidate
+// streams that offer each point once and whose results are discarded when
+// two kept distances are equal: admit if d < list[k-1], insert after the
+// elements smaller than d.
+template <int S>
+__device__ __forceinline__ void insert_sorted(WarpList<S>& L, float d, int p, int lane) {
+    if (!(d < L.kth)) return;
+    unsigned lt = 0;
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        lt += __popc(__ballot_sync(0xffffffffu, t < L.counter && L.dist[s] < d));
+    }
+    const int pos = (int)lt;
+    float pd[S];
+    int pi[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        float up_d = __shfl_up_sync(0xffffffffu, L.dist[s], 1);
+        int up_i = __shfl_up_sync(0xffffffffu, L.idx[s], 1);
+        float wrap_d = __shfl_sync(0xffffffffu, s > 0 ? L.dist[s > 0 ? s - 1 : 0] : 0.f, 31);
+        int wrap_i = __shfl_sync(0xffffffffu, s > 0 ? L.idx[s > 0 ? s - 1 : 0] : 0, 31);
+        pd[s] = lane == 0 ? wrap_d : up_d;
+        pi[s] = lane == 0 ? wrap_i : up_i;
+    }
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        if (t < L.k) {
+            if (t == pos) { L.dist[s] = d; L.idx[s] = p; }
+            else if (t > pos) { L.dist[s] = pd[s]; L.idx[s] = pi[s]; }
+        }
+    }
+    L.counter = L.counter == L.k ? L.k : L.counter + 1;
+    L.kth = L.fetch_dist(L.k - 1);
+}
+
+// Warp bitonic sort of one (d, p) pair per lane, ascending in d across lanes.
+__device__ __forceinline__ void warp_sort32(float& d, int& p, int lane) {
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const float od = __shfl_xor_sync(0xffffffffu, d, stride);
+            const int op = __shfl_xor_sync(0xffffffffu, p, stride);
+            const bool keep_min = ((lane & stride) == 0) == ((lane & size) == 0);
+            if (keep_min ? (od < d) : (od > d)) { d = od; p = op; }
+        }
+    }
+}
+
+// Value of slot m of the list, m chosen per lane.
+template <int S>
+__device__ __forceinline__ float list_dist_at(const WarpList<S>& L, int m) {
+    float v = 0.0f;
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const float u = __shfl_sync(0xffffffffu, L.dist[s], m & 31);
+        if ((m >> 5) == s) v = u;
+    }
+    return v;
+}
+
+// Merges the lanes' admitted candidates (ok) into the sorted list in one
+// step: the batch is sorted by a warp bitonic network, every element's slot
+// in the merged order is found by binary search in the other sequence, and
+// the merged prefix is exchanged through shared memory (sd/sp: 32*S slots
+// owned by the calling warp).  Equal distances place the list's element
+// first.  The result is the sorted L.k smallest of list + batch, like L.k
+// insert_sorted calls, so it serves the same (tie-free) candidate streams.
+template <int S>
+__device__ __forceinline__ void merge_batch(WarpList<S>& L, float d, int p, bool ok, int lane, float* sd, int* sp) {
+    float bd = ok ? d : 3.0e38f;
+    int bp = p;
+    const int nb = __popc(__ballot_sync(0xffffffffu, ok));
+    warp_sort32(bd, bp, lane);
+    const int cnt = L.counter, cap = L.k;
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        const float x = L.dist[s];
+        int lo = 0, hi = nb;  // batch elements < x
+#pragma unroll
+        for (int it = 0; it < 6; it++) {
+            const int mid = (lo + hi) >> 1;
+            const float v = __shfl_sync(0xffffffffu, bd, mid & 31);
+            if (lo < hi) {
+                if (v < x) lo = mid + 1;
+                else hi = mid;
+            }
+        }
+        const int r = t + lo;
+        if (t < cnt && r < cap) { sd[r] = x; sp[r] = L.idx[s]; }
+    }
+    {
+        int lo = 0, hi = cnt;  // list elements <= bd
+#pragma unroll
+        for (int it = 0; it < 9; it++) {  // cnt <= 256
+            const int mid = (lo + hi) >> 1;
+            const float v = list_dist_at(L, mid);
+            if (lo < hi) {
+                if (v <= bd) lo = mid + 1;
+                else hi = mid;
+            }
+        }
+        const int r = lane + lo;
+        if (lane < nb && r < cap) { sd[r] = bd; sp[r] = bp; }
+    }
+    __syncwarp();
+    const int nc = min(cnt + nb, cap);
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        if (t < nc) { L.dist[s] = sd[t]; L.idx[s] = sp[t]; }
+    }
+    __syncwarp();
+    L.counter = nc;
+    L.kth = L.fetch_dist(cap - 1);
+}
+
 // Locate cell (cx,cy,cz) of a level: returns [start,end) into the level's
 // order array, or start == end == -1 when the cell is empty / out of range.
 __device__ __forceinline__ int2 find_cell(const LevelDev& L, int cx, int cy, int cz) {

@@ -155,6 +155,32 @@ const int kShell[26][3] = {
 
 struct KnnStats { long long visited_points = 0; int max_level = 0; };
 
+// Continue decision on the last cube of a shell (GridKNNCuda.cu:694-741) for a
+// query whose list holds `counter` entries with k-th distance `kth`: true =
+// search the next shell.
+bool decide_more(const Grid& g, int q, int L, int o, int counter, int k, float kth, float thres) {
+    const int B = g.lv[L].B;
+    const float h = (g.b - g.a) / (float)B;
+    const int ci[3] = {g.cx[q] >> L, g.cy[q] >> L, g.cz[q] >> L};
+    const float c[3] = {g.x[q], g.y[q], g.z[q]};
+    const float xmin = g.a;
+    if (counter < k) {
+        const float st = std::sqrt(thres);
+        for (int d = 0; d < 3; d++) {
+            if (ci[d] - o >= 0 && st > face_lo(c[d], xmin, (float)(ci[d] - o), h)) return true;
+            if (ci[d] + o + 1 <= B && st > face_hi(c[d], xmin, (float)(ci[d] + o + 1), h)) return true;
+        }
+        return false;
+    }
+    const float r = std::sqrt(kth);
+    bool more = false;
+    for (int d = 0; d < 3; d++) {
+        if (ci[d] - o >= 0 && r >= face_lo(c[d], xmin, (float)(ci[d] - o), h)) more = true;
+        if (ci[d] + o + 1 <= B && r >= face_hi(c[d], xmin, (float)(ci[d] + o + 1), h)) more = true;
+    }
+    return more;
+}
+
 // One query of GRIDCUDAKNNSELF_COMPACT (GridKNNCuda.cu:2322-2586) with the
 // kernel body construct_neighbors_self_compact (GridKNNCuda.cu:647-743).
 // Returns the level reached (0..7, or 8 when the query ran out of levels).
@@ -164,7 +190,6 @@ int knn_query(const Grid& g, int q, int k, float thres, float* dist, int* idx, i
     counter = 0;
     invalid = false;
     const float xq = g.x[q], yq = g.y[q], zq = g.z[q];
-    const float xmin = g.a;
 
     auto visit = [&](int L, int cx, int cy, int cz) {
         const auto& lv = g.lv[L];
@@ -184,29 +209,9 @@ int knn_query(const Grid& g, int q, int k, float thres, float* dist, int* idx, i
             if (d <= thres) append(dist, idx, k, counter, d, p);
         }
     };
-    // Continue decision on the last cube of a shell (GridKNNCuda.cu:694-741).
     auto decide = [&](int L, int o) -> bool {
         if (invalid) return false;
-        const int B = g.lv[L].B;
-        const float h = (g.b - g.a) / (float)B;
-        const int xi = g.cx[q] >> L, yi = g.cy[q] >> L, zi = g.cz[q] >> L;
-        const float c[3] = {xq, yq, zq};
-        const int ci[3] = {xi, yi, zi};
-        if (counter < k) {
-            const float st = std::sqrt(thres);
-            for (int d = 0; d < 3; d++) {
-                if (ci[d] - o >= 0 && st > face_lo(c[d], xmin, (float)(ci[d] - o), h)) return true;
-                if (ci[d] + o + 1 <= B && st > face_hi(c[d], xmin, (float)(ci[d] + o + 1), h)) return true;
-            }
-            return false;
-        }
-        const float r = std::sqrt(dist[k - 1]);
-        bool more = false;
-        for (int d = 0; d < 3; d++) {
-            if (ci[d] - o >= 0 && r >= face_lo(c[d], xmin, (float)(ci[d] - o), h)) more = true;
-            if (ci[d] + o + 1 <= B && r >= face_hi(c[d], xmin, (float)(ci[d] + o + 1), h)) more = true;
-        }
-        return more;
+        return decide_more(g, q, L, o, counter, k, dist[k - 1], thres);
     };
 
     visit(0, g.cx[q], g.cy[q], g.cz[q]);
@@ -226,6 +231,175 @@ int knn_query(const Grid& g, int q, int k, float thres, float* dist, int* idx, i
     if (invalid)
         for (int i = 0; i < k; i++) idx[i] = -1;
     return reached;
+}
+
+// ---------------------------------------------------------------------------
+// Learned search proposal (an extension of this project; the reference has no
+// counterpart).  A proposal class names a box of level-L cells of half-width R
+// around the query's level-L cell; the last class means "run the plain search".
+// The box search keeps the k+1 smallest distances of the box and is accepted
+// only when it provably equals the plain search's list:
+//   (1) at least k candidates, and the k+1 smallest distances pairwise distinct
+//       (then any candidate order yields the same sorted list);
+//   (2) the k-th distance ball lies inside the box with a margin of 2e-6 in
+//       normalised units (all points outside the box are strictly farther), so
+//       the k smallest of the box are the k smallest of the cloud, G;
+//   (3) the plain search's stop step is replayed: for step s (own cell, then
+//       the ring at level s-1) the plain list equals G once the visited block
+//       holds G, so the decision there is decide_more(kth(G)); before that the
+//       plain k-th distance is >= kth(G) and the search continues whenever
+//       decide_more(kth(G)) and the under-full branch both say "continue";
+//   (4) no cell of a level the plain search visits holds >= MAX_PNTS_IN_CUBE
+//       points (the plain search would have marked the query invalid).
+// Any failed check falls back to the plain search.
+struct BoxClass { int level, radius; };
+constexpr int kProposalClasses = 16;
+const BoxClass kBox[kProposalClasses - 1] = {{0, 1}, {0, 2}, {0, 3}, {0, 4}, {0, 5}, {0, 6}, {1, 4}, {1, 5},
+                                             {1, 6}, {2, 4}, {2, 5}, {2, 6}, {3, 4}, {3, 5}, {3, 6}};
+constexpr double kBoxMargin = 2e-6;
+
+// points in cells [x0, x1] of row (cy, cz) at level L (clipped to the grid)
+int row_count(const Grid& g, int L, int x0, int x1, int cy, int cz) {
+    const auto& lv = g.lv[L];
+    if (cy < 0 || cy >= lv.B || cz < 0 || cz >= lv.B) return 0;
+    x0 = std::max(x0, 0);
+    x1 = std::min(x1, lv.B - 1);
+    if (x0 > x1) return 0;
+    const int base = cy * lv.B + cz * lv.B * lv.B;
+    auto i0 = std::lower_bound(lv.keys.begin(), lv.keys.end(), base + x0) - lv.keys.begin();
+    auto i1 = std::lower_bound(lv.keys.begin(), lv.keys.end(), base + x1 + 1) - lv.keys.begin();
+    return lv.start[i1] - lv.start[i0];
+}
+
+// 8 features: log2(1+count)/16 of the query's own cell at levels 0..5 and of
+// its 3x3x3 level-0 block, and twice the smallest fractional distance of the
+// query to a face of its level-0 cell.
+void proposal_features(const Grid& g, int q, float f[8]) {
+    for (int L = 0; L < 6; L++) {
+        const int c = row_count(g, L, g.cx[q] >> L, g.cx[q] >> L, g.cy[q] >> L, g.cz[q] >> L);
+        f[L] = std::log2(1.0f + (float)c) * 0.0625f;
+    }
+    int blk = 0;
+    for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++) blk += row_count(g, 0, g.cx[q] - 1, g.cx[q] + 1, g.cy[q] + dy, g.cz[q] + dz);
+    f[6] = std::log2(1.0f + (float)blk) * 0.0625f;
+    const float c[3] = {g.x[q], g.y[q], g.z[q]};
+    const int ci[3] = {g.cx[q], g.cy[q], g.cz[q]};
+    float m = 0.5f;
+    for (int d = 0; d < 3; d++) {
+        const float v = (c[d] - g.a) / (g.b - g.a) * (float)kBuckets;
+        const float fr = v - (float)ci[d];
+        m = std::min(m, std::min(fr, 1.0f - fr));
+    }
+    f[7] = 2.0f * std::max(m, 0.0f);
+}
+
+// Level-0 cell range [lo, end) per axis of the box of class `cls` whose
+// (y, z) half-width is `ryz` (<= radius) level-L cells.
+void box_bounds(const Grid& g, int q, int cls, int ryz, int lo[3], int end[3]) {
+    const int L = kBox[cls].level, R = kBox[cls].radius;
+    const int ci[3] = {g.cx[q] >> L, g.cy[q] >> L, g.cz[q] >> L};
+    for (int d = 0; d < 3; d++) {
+        const int r = d == 0 ? R : ryz;
+        lo[d] = (ci[d] - r) * (1 << L);
+        end[d] = (ci[d] + r + 1) * (1 << L);
+    }
+}
+
+// Condition (2): the ball of radius sqrt(kth) + margin is inside the box.
+bool ball_in_box(const Grid& g, int q, float kth, const int lo[3], const int end[3]) {
+    const double r = std::sqrt((double)kth) + kBoxMargin;
+    const double h0 = (double)((g.b - g.a) / (float)kBuckets);
+    const double c[3] = {g.x[q], g.y[q], g.z[q]};
+    for (int d = 0; d < 3; d++) {
+        if (lo[d] > 0 && !(r < c[d] - ((double)g.a + lo[d] * h0))) return false;
+        if (end[d] < kBuckets && !(r < ((double)g.a + end[d] * h0) - c[d])) return false;
+    }
+    return true;
+}
+
+// First plain-search step (0 = own cell, s = ring at level s-1) at which p is visited.
+int visit_step(const Grid& g, int q, int p) {
+    if (g.cx[p] == g.cx[q] && g.cy[p] == g.cy[q] && g.cz[p] == g.cz[q]) return 0;
+    for (int L = 0; L < kLevels; L++) {
+        if (std::abs((g.cx[p] >> L) - (g.cx[q] >> L)) <= 1 && std::abs((g.cy[p] >> L) - (g.cy[q] >> L)) <= 1 &&
+            std::abs((g.cz[p] >> L) - (g.cz[q] >> L)) <= 1)
+            return L + 1;
+    }
+    return kLevels + 1;
+}
+
+// Label of a query from the plain search's k-th distance: the cheapest class
+// whose box passes condition (2), else the plain class.
+int proposal_label(const Grid& g, int q, int counter, int k, float kth) {
+    if (counter < k) return kProposalClasses - 1;
+    for (int c = 0; c < kProposalClasses - 1; c++) {
+        int lo[3], end[3];
+        box_bounds(g, q, c, kBox[c].radius, lo, end);
+        if (ball_in_box(g, q, kth, lo, end)) return c;
+    }
+    return kProposalClasses - 1;
+}
+
+// Box search + certification for one query.  Returns true (and fills
+// idx[0..k), reached) when the box result is certified equal to the plain
+// search's; `visited` counts the candidates examined.
+bool box_query(const Grid& g, int q, int k, int cls, float thres, const int* maxpop, int* idx, int& reached,
+               long long& visited, std::vector<std::pair<float, int>>& cand) {
+    const int L = kBox[cls].level, R = kBox[cls].radius;
+    const auto& lv = g.lv[L];
+    const int ci[3] = {g.cx[q] >> L, g.cy[q] >> L, g.cz[q] >> L};
+    cand.clear();
+    for (int dz = -R; dz <= R; dz++)
+        for (int dy = -R; dy <= R; dy++) {
+            const int cy = ci[1] + dy, cz = ci[2] + dz;
+            if (cy < 0 || cy >= lv.B || cz < 0 || cz >= lv.B) continue;
+            const int x0 = std::max(ci[0] - R, 0), x1 = std::min(ci[0] + R, lv.B - 1);
+            const int base = cy * lv.B + cz * lv.B * lv.B;
+            auto i0 = std::lower_bound(lv.keys.begin(), lv.keys.end(), base + x0) - lv.keys.begin();
+            auto i1 = std::lower_bound(lv.keys.begin(), lv.keys.end(), base + x1 + 1) - lv.keys.begin();
+            for (int j = lv.start[i0]; j < lv.start[i1]; j++) {
+                const int p = lv.order[j];
+                if (p == q) continue;
+                const float d = dist3(g.x[q], g.y[q], g.z[q], g.x[p], g.y[p], g.z[p]);
+                visited++;
+                if (d <= thres) cand.push_back({d, p});
+            }
+        }
+    const int m = (int)cand.size();
+    if (m < k) return false;
+    const int keep = std::min(m, k + 1);
+    std::partial_sort(cand.begin(), cand.begin() + keep, cand.end(),
+                      [](const std::pair<float, int>& a, const std::pair<float, int>& b) { return a.first < b.first; });
+    for (int i = 1; i < keep; i++)                                     // (1)
+        if (!(cand[i - 1].first < cand[i].first)) return false;
+    const float kth = cand[k - 1].first;
+    int lo[3], end[3];
+    box_bounds(g, q, cls, R, lo, end);
+    if (!ball_in_box(g, q, kth, lo, end)) return false;                // (2)
+    int sg = 0;
+    for (int i = 0; i < k; i++) sg = std::max(sg, visit_step(g, q, cand[i].second));
+    int sf = -1;                                                       // (3)
+    for (int s = 0; s <= kLevels; s++) {
+        const int Ls = s == 0 ? 0 : s - 1, o = s == 0 ? 0 : 1;
+        const bool more = decide_more(g, q, Ls, o, k, k, kth, thres);
+        if (!more) { sf = s; break; }
+        if (!decide_more(g, q, Ls, o, 0, k, kth, thres)) return false;
+    }
+    if (sf < 0 || sg > sf) return false;
+    for (int l = 0; l <= std::max(sf - 1, 0); l++)                     // (4)
+        if (maxpop[l] >= kMaxPointsInCube) return false;
+    for (int i = 0; i < k; i++) idx[i] = cand[i].second;
+    reached = std::max(sf - 1, 0);
+    return true;
+}
+
+void level_maxpop(const Grid& g, int* maxpop) {
+    for (int L = 0; L < kLevels; L++) {
+        int m = 0;
+        for (size_t c = 0; c + 1 < g.lv[L].start.size(); c++) m = std::max(m, g.lv[L].start[c + 1] - g.lv[L].start[c]);
+        maxpop[L] = m;
+    }
 }
 
 // EGT predicate isEllipicGabrielNeighbor_GKNN (EGT_CUDA.cu:136-170) with its
@@ -525,6 +699,76 @@ int orc_knn(const float* xyz, int n, int k, int* lists, float* pos, int* perm, f
     }
     ext[0] = g.mn; ext[1] = g.mx;
     if (visited_total) *visited_total = visited_sum;
+    return invalid_count;
+}
+
+// Learned-proposal training data (extension, no reference counterpart):
+// features [n*8] and labels [n] of every query in sorted space, labels from
+// the plain search's k-th distance.  Returns the number of plain-class labels.
+int orc_proposal_data(const float* xyz, int n, int k, float* feats, uint8_t* labels) {
+    Grid g;
+    build_grid(xyz, n, g, kLevels);
+    float thres = 1e8f;
+    thres /= (g.mx - g.mn);
+    thres *= thres;
+    int plain = 0;
+#pragma omp parallel reduction(+ : plain)
+    {
+        std::vector<float> dist(k);
+        std::vector<int> idx(k);
+#pragma omp for schedule(dynamic, 256)
+        for (int q = 0; q < n; q++) {
+            int counter;
+            bool invalid;
+            long long visited = 0;
+            knn_query(g, q, k, thres, dist.data(), idx.data(), counter, invalid, visited);
+            proposal_features(g, q, feats + (size_t)q * 8);
+            const int lab = invalid ? kProposalClasses - 1 : proposal_label(g, q, counter, k, dist[k - 1]);
+            labels[q] = (uint8_t)lab;
+            plain += lab == kProposalClasses - 1;
+        }
+    }
+    return plain;
+}
+
+// Grid kNN through the proposal: per-query class `cls` [n] (sorted space);
+// class kProposalClasses-1 or a failed certification runs the plain search.
+// lists [n*k] must equal orc_knn's.  certified [n]: 1 = box result used.
+// Returns the number of invalid queries; box_visited/plain_visited count the
+// candidates examined by each part.
+int orc_knn_proposal(const float* xyz, int n, int k, const uint8_t* cls, int* lists, uint8_t* certified,
+                     int* level, long long* box_visited, long long* plain_visited) {
+    Grid g;
+    build_grid(xyz, n, g, kLevels);
+    float thres = 1e8f;
+    thres /= (g.mx - g.mn);
+    thres *= thres;
+    int maxpop[kLevels];
+    level_maxpop(g, maxpop);
+    int invalid_count = 0;
+    long long bv = 0, pv = 0;
+#pragma omp parallel reduction(+ : invalid_count, bv, pv)
+    {
+        std::vector<float> dist(k);
+        std::vector<std::pair<float, int>> cand;
+#pragma omp for schedule(dynamic, 256)
+        for (int q = 0; q < n; q++) {
+            int* out = lists + (size_t)q * k;
+            int reached = 0;
+            bool ok = false;
+            if (cls[q] < kProposalClasses - 1) ok = box_query(g, q, k, cls[q], thres, maxpop, out, reached, bv, cand);
+            if (!ok) {
+                int counter;
+                bool invalid;
+                reached = knn_query(g, q, k, thres, dist.data(), out, counter, invalid, pv);
+                if (invalid) invalid_count++;
+            }
+            certified[q] = ok ? 1 : 0;
+            if (level) level[q] = reached;
+        }
+    }
+    *box_visited = bv;
+    *plain_visited = pv;
     return invalid_count;
 }
 

@@ -44,6 +44,10 @@ def lib():
         L.orc_output.argtypes = [vp, vp, vp, i32, vp]
         L.orc_bruteforce.argtypes = [vp, i32, i32, vp, vp]
         L.orc_knn_timed.argtypes = [vp, i32, i32, i32, vp, vp]
+        L.orc_proposal_data.restype = i32
+        L.orc_proposal_data.argtypes = [vp, i32, i32, vp, vp]
+        L.orc_knn_proposal.restype = i32
+        L.orc_knn_proposal.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -154,3 +158,92 @@ def knn_timed(xyz: np.ndarray, k: int, stride: int):
     tb, tq = C.c_double(0), C.c_double(0)
     lib().orc_knn_timed(_p(xyz), xyz.shape[0], k, stride, C.byref(tb), C.byref(tq))
     return tb.value, tq.value
+
+
+# ---------------------------------------------------------------------------
+# Learned search proposal (extension of this project; no reference counterpart)
+
+PROPOSAL_CLASSES = 16
+PROPOSAL_BOXES = [(0, 1), (0, 2), (0, 3), (0, 4), (0, 5), (0, 6), (1, 4), (1, 5),
+                  (1, 6), (2, 4), (2, 5), (2, 6), (3, 4), (3, 5), (3, 6)]
+
+
+def proposal_data(xyz: np.ndarray, k: int):
+    """Features [n,8] and labels [n] (sorted space) from the plain grid kNN."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+    n = xyz.shape[0]
+    feats = np.empty((n, 8), np.float32)
+    labels = np.empty(n, np.uint8)
+    lib().orc_proposal_data(_p(xyz), n, k, _p(feats), _p(labels))
+    return feats, labels
+
+
+def knn_proposal(xyz: np.ndarray, k: int, cls: np.ndarray):
+    """Grid kNN driven by per-query proposal classes (sorted space).  The lists
+    must equal knn()'s; `certified` marks queries answered by the box search."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+    cls = np.ascontiguousarray(cls, dtype=np.uint8)
+    n = xyz.shape[0]
+    lists = np.empty((n, k), np.int32)
+    cert = np.empty(n, np.uint8)
+    level = np.empty(n, np.int32)
+    bv, pv = C.c_longlong(0), C.c_longlong(0)
+    inv = lib().orc_knn_proposal(_p(xyz), n, k, _p(cls), _p(lists), _p(cert), _p(level), C.byref(bv), C.byref(pv))
+    return dict(lists=lists, certified=cert, level=level, invalid=inv, box_visited=bv.value,
+                plain_visited=pv.value)
+
+
+# Proposal network (MLP 8 -> 32 -> 32 -> 16, ReLU, softmax), restated in float64
+# for checking the device kernels.  params: the binary16 parameter vector in
+# the layout W1[32][8] b1 W2[32][32] b2 W3[16][32] b3.
+def _mlp_unpack(params: np.ndarray):
+    params = np.asarray(params)
+    # binary16 parameter vectors are used at their binary16 values; float64
+    # vectors (finite-difference checks) as given
+    p = params.copy() if params.dtype == np.float64 else params.astype(np.float16).astype(np.float64)
+    sizes = [("W1", (32, 8)), ("b1", (32,)), ("W2", (32, 32)), ("b2", (32,)), ("W3", (16, 32)), ("b3", (16,))]
+    out, o = {}, 0
+    for name, shp in sizes:
+        m = int(np.prod(shp))
+        out[name] = p[o:o + m].reshape(shp)
+        o += m
+    assert o == p.size == 1872
+    return out
+
+
+def mlp_forward(params: np.ndarray, feats: np.ndarray):
+    """Returns (h1, h2, logits) for feats [m, 8]."""
+    P = _mlp_unpack(params)
+    x = np.asarray(feats, dtype=np.float64)
+    h1 = np.maximum(x @ P["W1"].T + P["b1"], 0.0)
+    h2 = np.maximum(h1 @ P["W2"].T + P["b2"], 0.0)
+    return h1, h2, h2 @ P["W3"].T + P["b3"]
+
+
+def mlp_loss_grad(params: np.ndarray, feats: np.ndarray, labels: np.ndarray):
+    """Mean cross-entropy and its gradient w.r.t. the parameter vector (float64)."""
+    P = _mlp_unpack(params)
+    x = np.asarray(feats, dtype=np.float64)
+    y = np.asarray(labels).astype(np.int64)
+    m = x.shape[0]
+    h1, h2, z = mlp_forward(params, x)
+    z = z - z.max(1, keepdims=True)
+    e = np.exp(z)
+    s = e.sum(1, keepdims=True)
+    loss = float(np.mean(np.log(s[:, 0]) - z[np.arange(m), y]))
+    d3 = e / s
+    d3[np.arange(m), y] -= 1.0
+    d3 /= m
+    d2 = (d3 @ P["W3"]) * (h2 > 0)
+    d1 = (d2 @ P["W2"]) * (h1 > 0)
+    g = np.concatenate([(d1.T @ x).ravel(), d1.sum(0), (d2.T @ h1).ravel(), d2.sum(0), (d3.T @ h2).ravel(),
+                        d3.sum(0)])
+    return loss, g
+
+
+def mlp_classes(params: np.ndarray, feats: np.ndarray, tau: float) -> np.ndarray:
+    """Smallest class whose cumulative softmax probability reaches tau."""
+    _, _, z = mlp_forward(params, feats)
+    e = np.exp(z - z.max(1, keepdims=True))
+    cdf = np.cumsum(e, 1) / e.sum(1, keepdims=True)
+    return np.minimum((cdf < tau).sum(1), 15).astype(np.uint8)

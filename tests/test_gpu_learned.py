@@ -1,0 +1,176 @@
+"""Learned search proposal on the GPU (extension; no reference counterpart).
+
+* features and labels computed by the device equal the oracle's;
+* the device training kernels' gradients equal the float64 oracle's;
+* training on labels from the plain search lowers the loss;
+* the proposal-driven kNN returns lists bit-identical to the plain kNN for a
+  trained network, an untrained one, any threshold and tie-heavy clouds;
+* and the trained network makes the search faster than the plain method.
+"""
+import numpy as np
+import pytest
+
+from multigpuegtsmoothing_b200 import datagen
+
+pytestmark = pytest.mark.gpu
+
+
+def _dense_dups():
+    g = np.random.default_rng(1)
+    a = (g.random((60000, 3), dtype=np.float32) * np.float32(0.05)).astype(np.float32)
+    return np.concatenate([a, a[:6000]])
+
+
+def _lattice():
+    t = np.arange(40, dtype=np.float32)
+    return np.stack(np.meshgrid(t, t, t, indexing="ij"), -1).reshape(-1, 3)
+
+
+@pytest.fixture(scope="module")
+def trained(capi):
+    """A proposal for k=40 trained on two 1M-point superquadric clouds."""
+    p = capi.SearchProposal(40, seed=11)
+    for seed in (100, 101):
+        g = capi.GridStructure(datagen.superquadrics(1_000_000, seed=seed))
+        g.GRIDCUDAKNNSELF_COMPACT(40)
+        p.collect(g, stride=1)
+        g.close()
+    losses = p.train(1500, batch=4096, lr=3e-3)
+    return p, losses
+
+
+def test_features_and_labels_match_oracle(capi, oracle):
+    xyz = datagen.sphere_cloud()
+    g = capi.GridStructure(xyz)
+    g.GRIDCUDAKNNSELF_COMPACT(40)
+    p = capi.SearchProposal(40, seed=5)
+    f, lab, cls = p.inspect(g)
+    of, olab = oracle.proposal_data(xyz, 40)
+    # log2 of the device and of the host library may differ in the last bit
+    assert np.abs(f - of).max() <= 2e-7
+    assert np.array_equal(lab, olab)
+    ocls = oracle.mlp_classes(p.params(), f, p.tau)
+    assert (cls == ocls).mean() > 0.999
+
+
+def test_gradients_match_oracle(capi, oracle):
+    xyz = datagen.sphere_cloud()
+    of, olab = oracle.proposal_data(xyz, 40)
+    rng = np.random.default_rng(3)
+    rows = rng.choice(of.shape[0], 3000, replace=False)
+    p = capi.SearchProposal(40, seed=9)
+    for rnd in range(2):
+        g, loss = p.gradients(of[rows], olab[rows])
+        oloss, og = oracle.mlp_loss_grad(p.params(), of[rows], olab[rows])
+        assert abs(loss - oloss) <= 1e-5 * max(1.0, abs(oloss))
+        scale = np.abs(og).max()
+        assert np.abs(g - og).max() <= 1e-4 * scale, (rnd, np.abs(g - og).max(), scale)
+        # move the parameters and check again
+        g2 = capi.GridStructure(xyz)
+        g2.GRIDCUDAKNNSELF_COMPACT(40)
+        p.collect(g2)
+        p.train(50, batch=2048, lr=1e-2)
+        g2.close()
+
+
+def test_training_lowers_loss(trained):
+    _, losses = trained
+    assert np.all(np.isfinite(losses))
+    assert losses[-100:].mean() < 0.75 * losses[:5].mean()
+
+
+@pytest.mark.parametrize("case,k", [("sphere", 40), ("dups", 12), ("lattice", 26), ("superquadrics", 40)])
+def test_learned_lists_bit_identical(capi, trained, case, k):
+    xyz = {"sphere": lambda: datagen.sphere_cloud(), "dups": _dense_dups, "lattice": _lattice,
+           "superquadrics": lambda: datagen.superquadrics(400_000, seed=7)}[case]()
+    g = capi.GridStructure(xyz)
+    g.GRIDCUDAKNNSELF_COMPACT(k)
+    plain = g.sorted_lists()
+    t_plain = g.timings()
+    proposals = [capi.SearchProposal(k, seed=1)]
+    if k == 40:
+        proposals.append(trained[0])
+    for p in proposals:
+        for tau in (0.3, 0.85, 1.0):
+            p.tau = tau
+            g.GRIDCUDAKNNSELF_LEARNED(k, p)
+            assert np.array_equal(g.sorted_lists(), plain), (case, tau)
+            t = g.timings()
+            assert t["invalid_queries"] == t_plain["invalid_queries"]
+            assert t["levels_used"] == t_plain["levels_used"]
+            assert 0 <= t["certified_queries"] <= t["box_queries"] <= xyz.shape[0]
+    p = trained[0]
+    p.tau = 0.85
+    if case == "lattice":
+        g.GRIDCUDAKNNSELF_LEARNED(k, proposals[0])
+        assert g.timings()["certified_queries"] == 0  # every lattice box has ties
+    if case == "superquadrics":
+        g.GRIDCUDAKNNSELF_LEARNED(k, p)
+        t = g.timings()
+        assert t["certified_queries"] > 0.8 * xyz.shape[0]
+    g.close()
+
+
+def test_learned_beats_plain(capi, trained):
+    p, _ = trained
+    p.tau = 0.85
+    g = capi.GridStructure(datagen.superquadrics(2_000_000, seed=3))
+    best = {"plain": 1e30, "learned": 1e30}
+    for _ in range(3):
+        g.GRIDCUDAKNNSELF_COMPACT(40)
+        best["plain"] = min(best["plain"], g.timings()["knn_ms"])
+        plain = g.sorted_lists() if _ == 0 else plain
+        g.GRIDCUDAKNNSELF_LEARNED(40, p)
+        best["learned"] = min(best["learned"], g.timings()["knn_ms"])
+    assert np.array_equal(g.sorted_lists(), plain)
+    speedup = best["plain"] / best["learned"]
+    print(f"learned proposal speed-up over the plain search: {speedup:.2f}x "
+          f"(plain {best['plain']:.2f} ms, learned {best['learned']:.2f} ms)")
+    assert speedup > 1.0
+    g.close()
+
+
+def test_knn_mode_learned_through_egt_knn(capi, trained):
+    p, _ = trained
+    xyz = datagen.superquadrics(200_000, seed=8)
+    g = capi.GridStructure(xyz)
+    g.GRIDCUDAKNNSELF_COMPACT(40)
+    plain = g.sorted_lists()
+    g.close()
+    cfg = capi.default_config(knn_mode=1)
+    g = capi.GridStructure(xyz, config=cfg)
+    with pytest.raises(capi.EgtError):
+        g.GRIDCUDAKNNSELF_COMPACT(40)  # learned mode without a proposal
+    capi._check(capi.lib().egt_attach_proposal(g.handle, p.handle))
+    g.GRIDCUDAKNNSELF_COMPACT(40)
+    assert np.array_equal(g.sorted_lists(), plain)
+    assert g.timings()["box_queries"] > 0
+    g.close()
+
+
+def test_proposal_bad_arguments(capi):
+    p = capi.SearchProposal(40)
+    with pytest.raises(capi.EgtError):
+        p.train(10)  # no samples
+    with pytest.raises(capi.EgtError):
+        p.tau = 1.5
+    g = capi.GridStructure(datagen.sphere_cloud())
+    g.GRIDCUDAKNNSELF_COMPACT(20)
+    with pytest.raises(capi.EgtError):
+        g.GRIDCUDAKNNSELF_LEARNED(20, p)  # k differs from the proposal's
+    with pytest.raises(capi.EgtError):
+        p.collect(g)  # the handle's k differs
+    with pytest.raises(capi.EgtError):
+        capi.SearchProposal(0)
+    g.close()
+
+
+def test_plain_tie_rerun_is_exercised(capi, oracle):
+    # the lattice has equal distances everywhere: the plain kernel must take
+    # its exact re-run path and still match the oracle
+    xyz = _lattice()
+    g = capi.GridStructure(xyz)
+    g.GRIDCUDAKNNSELF_COMPACT(26)
+    assert g.timings()["exact_reruns"] > 0
+    assert np.array_equal(g.sorted_lists(), oracle.knn(xyz, 26)["lists"])
+    g.close()
