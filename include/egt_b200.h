@@ -209,6 +209,46 @@ egt_status egt_knn_learned(egt_handle* h, int k, const egt_proposal* p, void* st
  * The proposal must outlive the attachment. */
 egt_status egt_attach_proposal(egt_handle* h, const egt_proposal* p);
 
+/* ---- Batched clouds (no reference counterpart) -------------------------------
+ * Many independent point clouds through the same path, each with its own k and
+ * its own normalisation cube and cell grid exactly as if it were a separate
+ * egt_create_cloud handle, so every cloud's lists and positions are identical
+ * to that handle's.  Each stage runs as one launch over all clouds: one sort
+ * per hierarchy level over (cloud, cell) keys, one persistent kNN kernel
+ * claiming query chunks of any cloud, one EGT kernel, and the Taubin loop over
+ * the union of the clouds' neighbourhoods as one captured CUDA graph.  An
+ * autotuner (first egt_batch_run, cached per size bucket and k) picks the kNN
+ * work chunk and the Taubin half-step kernel by timing them on the batch. */
+typedef struct egt_batch egt_batch;
+typedef struct egt_batch_timings {
+    float grid_ms, knn_ms, egt_ms, taubin_ms, output_ms, tune_ms;
+    int clouds;
+    int64_t points;
+    int64_t invalid_queries;  /* over all clouds */
+    int64_t exact_reruns;     /* kNN queries re-searched with the one-at-a-time rule */
+    int64_t csr_nnz;          /* kept neighbours over all clouds */
+    int knn_chunk;            /* queries per work claim (autotuned) */
+    int taubin_mode;          /* 0 staged tiles, 1 direct gathers (autotuned) */
+} egt_batch_timings;
+/* count clouds concatenated in xyz_host ([offsets[count]][3] AoS float),
+ * cloud c = points [offsets[c], offsets[c+1]) with k[c] neighbours (1..255). */
+egt_status egt_batch_create(const float* xyz_host, const int64_t* offsets, const int* k, int count,
+                            const egt_config* cfg, void* stream, egt_batch** out);
+egt_status egt_batch_knn(egt_batch* b, void* stream);
+egt_status egt_batch_filter(egt_batch* b, float alpha, void* stream);
+egt_status egt_batch_taubin(egt_batch* b, int iters, float lambda, float mu, void* stream);
+/* Autotune (first call) + kNN + EGT filter + Taubin, always starting from the
+ * input positions (the stage calls above work on the current positions). */
+egt_status egt_batch_run(egt_batch* b, int iters, float lambda, float mu, float alpha, void* stream);
+/* Fixes the tuning (knn_chunk >= 1, taubin_mode 0/1) instead of autotuning. */
+egt_status egt_batch_set_tuning(egt_batch* b, int knn_chunk, int taubin_mode);
+/* Denormalised positions of all clouds, original order, [offsets[count]][3] AoS host. */
+egt_status egt_batch_output(egt_batch* b, float* xyz_host, void* stream);
+/* Lists of one cloud like egt_get_knn_host: n_c*k_c ints, original ids and order. */
+egt_status egt_batch_get_knn_host(egt_batch* b, int cloud, int* lists_host);
+egt_status egt_batch_get_timings(egt_batch* b, egt_batch_timings* t);
+void egt_batch_destroy(egt_batch* b);
+
 /* Copies bytes from device memory (e.g. a pointer from egt_get_views) to host
  * memory after synchronising the handle's stream.  No reference counterpart:
  * lets hosts without their own CUDA runtime binding read the device views. */

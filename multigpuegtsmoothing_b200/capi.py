@@ -62,6 +62,16 @@ class Timings(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class BatchTimings(C.Structure):
+    _fields_ = [("grid_ms", C.c_float), ("knn_ms", C.c_float), ("egt_ms", C.c_float), ("taubin_ms", C.c_float),
+                ("output_ms", C.c_float), ("tune_ms", C.c_float), ("clouds", C.c_int), ("points", C.c_int64),
+                ("invalid_queries", C.c_int64), ("exact_reruns", C.c_int64), ("csr_nnz", C.c_int64),
+                ("knn_chunk", C.c_int), ("taubin_mode", C.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -112,6 +122,16 @@ def lib() -> C.CDLL:
             "egt_proposal_inspect": (i32, [vp, vp, vp, vp, vp]),
             "egt_knn_learned": (i32, [vp, i32, vp, vp]),
             "egt_attach_proposal": (i32, [vp, vp]),
+            "egt_batch_create": (i32, [vp, vp, vp, i32, C.POINTER(Config), vp, hp]),
+            "egt_batch_knn": (i32, [vp, vp]),
+            "egt_batch_filter": (i32, [vp, f32, vp]),
+            "egt_batch_taubin": (i32, [vp, i32, f32, f32, vp]),
+            "egt_batch_run": (i32, [vp, i32, f32, f32, f32, vp]),
+            "egt_batch_set_tuning": (i32, [vp, i32, i32]),
+            "egt_batch_output": (i32, [vp, vp, vp]),
+            "egt_batch_get_knn_host": (i32, [vp, i32, vp]),
+            "egt_batch_get_timings": (i32, [vp, C.POINTER(BatchTimings)]),
+            "egt_batch_destroy": (None, [vp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -440,3 +460,72 @@ class SearchProposal:
         _check(lib().egt_proposal_inspect(self.handle, provider.handle, None if f is None else _ptr(f),
                                           None if l is None else _ptr(l), None if c is None else _ptr(c)))
         return f, l, c
+
+
+class Batch:
+    """Many independent clouds through kNN -> EGT -> Taubin with one launch per
+    stage (egt_batch_*; no reference counterpart).  Each cloud's results equal
+    those of its own GridStructure run through the same calls."""
+
+    def __init__(self, clouds, config: Optional[Config] = None, stream: int = 0):
+        xyzs = [np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3) for x, _ in clouds]
+        ks = np.ascontiguousarray([int(k) for _, k in clouds], dtype=np.int32)
+        self.offsets = np.zeros(len(xyzs) + 1, np.int64)
+        self.offsets[1:] = np.cumsum([x.shape[0] for x in xyzs])
+        self.k = ks
+        allx = np.ascontiguousarray(np.concatenate(xyzs), dtype=np.float32)
+        cfg = config or default_config()
+        h = C.c_void_p()
+        self.stream = C.c_void_p(stream) if stream else None
+        _check(lib().egt_batch_create(_ptr(allx), _ptr(self.offsets), _ptr(ks), len(xyzs), C.byref(cfg), self.stream,
+                                      C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise EgtError(-5, "batch destroyed")
+        return self._h
+
+    def close(self):
+        if self._h is not None:
+            lib().egt_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def knn(self):
+        _check(lib().egt_batch_knn(self.handle, self.stream))
+
+    def filter(self, alpha: float):
+        _check(lib().egt_batch_filter(self.handle, float(alpha), self.stream))
+
+    def taubin(self, iters: int, lambda_: float = 0.63, mu: float = -0.64):
+        _check(lib().egt_batch_taubin(self.handle, int(iters), float(lambda_), float(mu), self.stream))
+
+    def run(self, iters: int = 150, lambda_: float = 0.63, mu: float = -0.64, alpha: float = 0.65):
+        _check(lib().egt_batch_run(self.handle, int(iters), float(lambda_), float(mu), float(alpha), self.stream))
+
+    def set_tuning(self, knn_chunk: int, taubin_mode: int):
+        _check(lib().egt_batch_set_tuning(self.handle, int(knn_chunk), int(taubin_mode)))
+
+    def output(self):
+        """List of per-cloud (n_c, 3) float32 positions in original order."""
+        out = np.empty((int(self.offsets[-1]), 3), np.float32)
+        _check(lib().egt_batch_output(self.handle, _ptr(out), self.stream))
+        return [out[self.offsets[c]:self.offsets[c + 1]] for c in range(len(self.k))]
+
+    def knn_host(self, cloud: int) -> np.ndarray:
+        n = int(self.offsets[cloud + 1] - self.offsets[cloud])
+        out = np.empty((n, int(self.k[cloud])), np.int32)
+        _check(lib().egt_batch_get_knn_host(self.handle, int(cloud), _ptr(out)))
+        return out
+
+    def timings(self) -> dict:
+        t = BatchTimings()
+        _check(lib().egt_batch_get_timings(self.handle, C.byref(t)))
+        return t.as_dict()

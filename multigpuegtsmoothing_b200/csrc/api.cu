@@ -76,6 +76,41 @@ egt_status warm_pool(int device) {
     return EGT_OK;
 }
 
+}  // namespace
+
+// A handle with the per-point buffers of n points and no grid (used by the
+// batch, which builds its own per-cloud grids).
+egt_status egt::new_bare_handle(const egt_config& cfg, int64_t n, cudaStream_t stream, egt_handle** out) {
+    *out = nullptr;
+    EGT_CUDA_TRY(cudaSetDevice(cfg.device));
+    EGT_TRY(::warm_pool(cfg.device));
+    egt_handle* h = new egt_handle();
+    h->cfg = cfg;
+    h->n = n;
+    h->stream = stream;
+    cudaError_t e = dev_alloc(h, &h->p4, sizeof(float4) * n);
+    if (e == cudaSuccess) e = dev_alloc(h, &h->x, sizeof(float) * n);
+    if (e == cudaSuccess) e = dev_alloc(h, &h->y, sizeof(float) * n);
+    if (e == cudaSuccess) e = dev_alloc(h, &h->z, sizeof(float) * n);
+    if (e == cudaSuccess) e = dev_alloc(h, &h->cell0, sizeof(uint32_t) * n);
+    if (e == cudaSuccess) e = dev_alloc(h, &h->perm, sizeof(int) * n);
+    if (e == cudaSuccess) e = dev_alloc(h, &h->d_counters, sizeof(unsigned long long) * kCtrWords);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * kCtrWords, h->stream);
+    for (auto& ev : h->ev)
+        if (e == cudaSuccess) e = cudaEventCreate(&ev);
+    if (e != cudaSuccess) {
+        set_error(cuda_msg(e, "new_bare_handle", __FILE__, __LINE__));
+        free_handle(h);
+        return e == cudaErrorMemoryAllocation ? EGT_ERR_NOMEM : EGT_ERR_CUDA;
+    }
+    *out = h;
+    return EGT_OK;
+}
+
+void egt::delete_handle(egt_handle* h) { free_handle(h); }
+
+namespace {
+
 egt_status create_common(const float* xyz, bool xyz_on_device, int64_t n, const uint32_t* tris, int64_t t,
                          const egt_config* cfg_in, void* stream, egt_handle** out) {
     if (!out) { set_error("null output handle pointer"); return EGT_ERR_ARG; }

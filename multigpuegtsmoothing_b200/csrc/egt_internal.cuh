@@ -187,6 +187,11 @@ struct egt_handle {
     int taubin_iters = -1;
     float taubin_lambda = 0.f, taubin_mu = 0.f;
     const void* taubin_key[4] = {};
+    int taubin_mode = 0;         // 0: staged tiles, 1: direct gathers (chosen by the batch autotuner)
+    int taubin_graph_mode = -1;  // mode the cached graph was captured with
+    // batched clouds: per-point cloud id (sorted order), bits of the largest id
+    const uint16_t* cloud_of = nullptr;
+    int cloud_bits = 0;
     // timing
     cudaEvent_t ev[16] = {};
     egt_timings tm{};
@@ -221,4 +226,6 @@ egt_status run_output(egt_handle* h, float* x, float* y, float* z);  // device o
 egt_status lists_original(egt_handle* h, int* out_dev);
 egt_status scatter_original(egt_handle* h, const float* soa_sorted, float* soa_orig);
 float elapsed_ms(cudaEvent_t a, cudaEvent_t b);
+egt_status new_bare_handle(const egt_config& cfg, int64_t n, cudaStream_t stream, egt_handle** out);
+void delete_handle(egt_handle* h);
 }  // namespace egt

@@ -20,17 +20,10 @@
 // rounding; the hierarchy therefore never re-reads positions.
 #include <cub/cub.cuh>
 #include "egt_internal.cuh"
+#include "grid_common.cuh"
 
 namespace egt {
 namespace {
-
-__device__ __forceinline__ uint32_t f2ord(float f) {
-    uint32_t u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float ord2f(uint32_t u) {
-    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
-}
 
 // Per-axis min/max over AoS xyz (the six thrust::reduce calls of
 // GridKNNCuda.cu:1042-1065 fused into one pass).
@@ -65,31 +58,9 @@ __global__ void k_init_extents(uint32_t* acc) {
     else if (threadIdx.x < 6) acc[threadIdx.x] = 0u;
 }
 
-// Scalar cube of InitStructure: thrust::reduce(.., 1e8f, minimum) - 1e-6f and
-// thrust::reduce(.., -1e8f, maximum) + 1e-6f per axis, then min/max over axes.
+// Scalar cube of InitStructure (finalize_norm in grid_common.cuh).
 __global__ void k_finalize_norm(const uint32_t* acc, float eps, float thres0, int64_t n, NormParams* out) {
-    float lo[3], hi[3];
-    for (int d = 0; d < 3; d++) {
-        lo[d] = __fsub_rn(fminf(1e8f, ord2f(acc[d])), 1e-6f);
-        hi[d] = __fadd_rn(fmaxf(-1e8f, ord2f(acc[3 + d])), 1e-6f);
-    }
-    float mn = lo[0], mx = hi[0];
-    // std::min / std::max semantics (returns the first argument on ties)
-    mn = (lo[1] < mn) ? lo[1] : mn;
-    mn = (lo[2] < mn) ? lo[2] : mn;
-    mx = (mx < hi[1]) ? hi[1] : mx;
-    mx = (mx < hi[2]) ? hi[2] : mx;
-    NormParams p;
-    p.mn = mn;
-    p.mx = mx;
-    p.a = -eps;
-    p.b = (float)(1.0 + (double)eps);
-    float t = thres0;
-    t = __fdiv_rn(t, __fsub_rn(mx, mn));
-    t = __fmul_rn(t, t);
-    p.thres = t;
-    p.n = (int)n;
-    *out = p;
+    *out = finalize_norm(acc, eps, thres0, n);
 }
 
 // normalize_points (GridKNNCuda.cu:840-849) + get_buckets_no_binary at B=1024

@@ -1,0 +1,248 @@
+// Device side of the exact grid kNN search, shared by the single-cloud kernels
+// (knn.cu) and the batched kernels (batch.cu).  See knn.cu for the reference
+// correspondence and the design.
+#pragma once
+#include "egt_internal.cuh"
+#include "knn_common.cuh"
+
+namespace egt {
+namespace {
+
+struct KnnArgs {
+    const float4* __restrict__ p4;
+    const NormParams* __restrict__ np;
+    LevelDev lv[kMaxLevels];
+    int n, k, max_pts;
+    int chunk;  // queries claimed per atomic by the persistent kernels
+    int* __restrict__ lists;
+    float* __restrict__ kth_out;
+    uint8_t* __restrict__ qlevel;
+    unsigned long long* __restrict__ counters;
+};
+
+constexpr int kWarps = 8;
+// The search kernels are latency-bound: keep four blocks (32 warps) resident
+// per SM, which caps them at 64 registers.
+constexpr int kMinBlocks = 4;
+
+// Continue decision after the last cube of a shell (GridKNNCuda.cu:694-741).
+__device__ __forceinline__ bool decide(const NormParams& np, int L, int o, int counter, int k, float kth,
+                                       bool invalid, float4 q, int cx0, int cy0, int cz0) {
+    if (invalid) return false;
+    const int B = 1024 >> L;
+    const float h = __fdiv_rn(__fsub_rn(np.b, np.a), (float)B);
+    const float c[3] = {q.x, q.y, q.z};
+    const int ci[3] = {cx0 >> L, cy0 >> L, cz0 >> L};
+    if (counter < k) {
+        const float st = __fsqrt_rn(np.thres);
+        bool more = false;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            more |= (ci[d] - o >= 0) && st > fs_face_lo(c[d], np.a, (float)(ci[d] - o), h);
+            more |= (ci[d] + o + 1 <= B) && st > fs_face_hi(c[d], np.a, (float)(ci[d] + o + 1), h);
+        }
+        return more;
+    }
+    const float r = __fsqrt_rn(kth);
+    bool more = false;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        more |= (ci[d] - o >= 0) && r >= fs_face_lo(c[d], np.a, (float)(ci[d] - o), h);
+        more |= (ci[d] + o + 1 <= B) && r >= fs_face_hi(c[d], np.a, (float)(ci[d] + o + 1), h);
+    }
+    return more;
+}
+
+// Batches admitting at least this many candidates are merged in one step.
+#ifndef EGT_KNN_MERGE_MIN
+#define EGT_KNN_MERGE_MIN 3
+#endif
+constexpr int kMergeMin = EGT_KNN_MERGE_MIN;
+
+// Offers one batch of candidates (one per lane, `adm` = admitted: d <= thres
+// and d < the list's last slot) to the list.
+//   kExact: the reference's appendDistanceGrid rule, one candidate at a time
+//           in lane order (dedup, FindPosition on equal distances);
+//   else:   sorted insertion, or one merge step for larger batches.  The two
+//           agree whenever the kept distances are pairwise distinct; callers
+//           discard results with equal distances (has_ties).
+template <bool kExact, int S>
+__device__ __forceinline__ void offer(WarpList<S>& L, float d, int p, bool adm, int lane, float* s_md, int* s_mp) {
+    unsigned mask = __ballot_sync(0xffffffffu, adm);
+    if (!kExact && __popc(mask) >= kMergeMin) {
+        merge_batch(L, d, p, adm, lane, s_md, s_mp);
+        return;
+    }
+    while (mask) {
+        const int src = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const float dd = __shfl_sync(0xffffffffu, d, src);
+        const int pp = __shfl_sync(0xffffffffu, p, src);
+        if (kExact) L.insert(dd, pp, lane);
+        else insert_sorted(L, dd, pp, lane);
+    }
+}
+
+// True when two of the first `keep` slots hold equal distances.
+template <int S>
+__device__ __forceinline__ bool has_ties(const WarpList<S>& L, int keep, int lane) {
+    bool bad = false;
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        const float up = __shfl_up_sync(0xffffffffu, L.dist[s], 1);
+        const float wrap = __shfl_sync(0xffffffffu, s > 0 ? L.dist[s > 0 ? s - 1 : 0] : 0.f, 31);
+        const float prev = lane == 0 ? wrap : up;
+        if (t >= 1 && t < keep && !(prev < L.dist[s])) bad = true;
+    }
+    return __any_sync(0xffffffffu, bad);
+}
+
+// Streams the points of `m` cells (cell l held by lane l as [cs, ce), ce < 0 =
+// empty) through the list, in cell order.  Sets `invalid` when a visited cell
+// holds >= max_pts points (GridKNNCuda.cu:672, 685): the cells before it are
+// still processed, the rest are not.  skipL >= 0: skip points whose level-skipL
+// cell lies in the 3x3x3 block around the query's (already visited).
+template <bool kExact, int S>
+__device__ __forceinline__ void stream_cells(WarpList<S>& L, bool& invalid, int m, int cs, int ce,
+                                             const int* __restrict__ order, const float4* __restrict__ p4,
+                                             int q, float4 pq, float thres, int max_pts, int lane,
+                                             int skipL, uint32_t qc0, int* s_pref, int* s_start, float* s_md,
+                                             int* s_mp) {
+    const bool exists = lane < m && ce >= 0;
+    const bool big = exists && (ce - cs) >= max_pts;
+    const unsigned bigmask = __ballot_sync(0xffffffffu, big);
+    const int mlim = bigmask ? (__ffs(bigmask) - 1) : m;
+    int sz = (lane < mlim && exists) ? ce - cs : 0;
+    int incl = sz;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    __syncwarp();
+    s_pref[lane] = incl;
+    s_start[lane] = cs;
+    __syncwarp();
+    const int qx = (int)((qc0 & 1023u) >> max(skipL, 0)), qy = (int)(((qc0 >> 10) & 1023u) >> max(skipL, 0)),
+              qz = (int)(((qc0 >> 20) & 1023u) >> max(skipL, 0));
+    for (int base = 0; base < total; base += 32) {
+        const int j = base + lane;
+        float d = 1e30f;
+        int p = -1;
+        bool ok = false;
+        if (j < total) {
+            int lo = 0, hi = mlim - 1;  // first cell with incl > j
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (s_pref[mid] > j) hi = mid;
+                else lo = mid + 1;
+            }
+            const int excl = lo > 0 ? s_pref[lo - 1] : 0;
+            const int pos = s_start[lo] + (j - excl);
+            p = order ? order[pos] : pos;
+            if (p != q) {
+                const float4 v = p4[p];
+                bool fresh = true;
+                if (skipL >= 0) {
+                    const uint32_t c = __float_as_uint(v.w);
+                    const int px = (int)((c & 1023u) >> skipL), py = (int)(((c >> 10) & 1023u) >> skipL),
+                              pz = (int)(((c >> 20) & 1023u) >> skipL);
+                    fresh = abs(px - qx) > 1 || abs(py - qy) > 1 || abs(pz - qz) > 1;
+                }
+                if (fresh) {
+                    d = fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z);
+                    ok = d <= thres;
+                }
+            }
+        }
+        offer<kExact, S>(L, d, p, ok && d < L.kth, lane, s_md, s_mp);
+    }
+    if (bigmask) invalid = true;
+}
+
+// The whole reference search for query q.  Returns the level reached
+// (kMaxLevels when the query ran out of levels).  kExact keeps the k-slot
+// list of the reference's insertion rule; otherwise the list keeps k+1 slots
+// (one more than the output) so that has_ties can check the k-th/(k+1)-th
+// boundary.  Either way the decisions see the k-th smallest distance offered
+// so far, which does not depend on the insertion rule.
+template <bool kExact, int S>
+__device__ int search(const KnnArgs& a, const NormParams& np, int q, float4 pq, WarpList<S>& L,
+                      bool& invalid, int lane, int* s_pref, int* s_start, float* s_md, int* s_mp) {
+    const uint32_t c0 = __float_as_uint(pq.w);
+    const int cx0 = c0 & 1023, cy0 = (c0 >> 10) & 1023, cz0 = (c0 >> 20) & 1023;
+    const int k = a.k;
+    L.init(kExact ? k : k + 1);
+    invalid = false;
+    // offset 0 at level 0: the query's own cell (always occupied)
+    int2 own = lane == 0 ? find_cell(a.lv[0], cx0, cy0, cz0) : make_int2(-1, -1);
+    stream_cells<kExact, S>(L, invalid, 1, own.x, own.y, nullptr, a.p4, q, pq, np.thres, a.max_pts, lane, -1, c0,
+                            s_pref, s_start, s_md, s_mp);
+    bool cont = decide(np, 0, 0, L.counter, k, kExact ? L.kth : L.fetch_dist(k - 1), invalid, pq, cx0, cy0, cz0);
+    int reached = 0;
+    for (int lvl = 0; cont; lvl++) {
+        reached = lvl;
+        const LevelDev& LV = a.lv[lvl];
+        int2 cell = make_int2(-1, -1);
+        if (lane < 26)
+            cell = find_cell(LV, (cx0 >> lvl) + kShell[lane][0], (cy0 >> lvl) + kShell[lane][1],
+                             (cz0 >> lvl) + kShell[lane][2]);
+        stream_cells<kExact, S>(L, invalid, 26, cell.x, cell.y, LV.order, a.p4, q, pq, np.thres, a.max_pts, lane,
+                                lvl - 1, c0, s_pref, s_start, s_md, s_mp);
+        cont = decide(np, lvl, 1, L.counter, k, kExact ? L.kth : L.fetch_dist(k - 1), invalid, pq, cx0, cy0, cz0);
+        if (lvl == kMaxLevels - 1) break;
+    }
+    // still searching after the B = 8 ring: invalid (GridKNNCuda.cu:2572-2586)
+    if (cont) { invalid = true; reached = kMaxLevels; }
+    return reached;
+}
+
+// One query of the plain search: the fast list rule first; if the k+1 kept
+// distances are not pairwise distinct the order of equal distances matters
+// and the query is searched again with the reference's exact rule.
+template <bool kFast, int S>
+__device__ __forceinline__ int plain_query(const KnnArgs& a, const NormParams& np, int q, float4 pq, WarpList<S>& L,
+                                           bool& invalid, int lane, int* s_pref, int* s_start, float* s_md,
+                                           int* s_mp, bool& rerun) {
+    rerun = false;
+    if (kFast) {
+        const int reached = search<false, S>(a, np, q, pq, L, invalid, lane, s_pref, s_start, s_md, s_mp);
+        if (!has_ties(L, min(L.counter, a.k + 1), lane)) return reached;
+        rerun = true;
+    }
+    return search<true, S>(a, np, q, pq, L, invalid, lane, s_pref, s_start, s_md, s_mp);
+}
+
+// Writes the outputs of query q from its final list.
+template <int S>
+__device__ __forceinline__ void write_query(const KnnArgs& a, int q, const WarpList<S>& L, bool invalid, int reached,
+                                            int lane) {
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        if (t < a.k) a.lists[(size_t)q * a.k + t] = invalid ? -1 : L.idx[s];
+    }
+    const float kth = L.fetch_dist(a.k - 1);
+    if (lane == 0) {
+        if (a.kth_out) a.kth_out[q] = (!invalid && L.counter >= a.k) ? kth : 1e10f;
+        if (a.qlevel) a.qlevel[q] = (uint8_t)reached;
+        if (invalid) atomicAdd(&a.counters[kCtrInvalid], 1ull);
+        atomicMax(&a.counters[kCtrMaxLevel], (unsigned long long)reached);
+    }
+}
+
+// Default number of queries a warp of the persistent kNN kernels claims per
+// atomic (KnnArgs::chunk).
+constexpr int kChunk = 4;
+
+// Next chunk of queries for the calling warp (uniform); >= n when done.
+__device__ __forceinline__ int claim(const KnnArgs& a, int lane) {
+    unsigned long long q0 = 0;
+    if (lane == 0) q0 = atomicAdd(&a.counters[kCtrWork], (unsigned long long)a.chunk);
+    return (int)min(__shfl_sync(0xffffffffu, q0, 0), (unsigned long long)a.n);
+}
+
+}  // namespace
+}  // namespace egt

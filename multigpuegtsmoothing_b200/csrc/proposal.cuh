@@ -101,7 +101,7 @@ __device__ __forceinline__ void box_bounds(int cls, int ryz, uint32_t c0, int lo
 __device__ __forceinline__ bool ball_in_box(const NormParams& np, float4 pq, float kth, const int lo[3],
                                             const int end[3]) {
     const double r = sqrt((double)kth) + kBoxMargin;
-    const double h0 = (double)__fdiv_rn(__fsub_rn(np.b, np.a), 1024.0f);
+    const double h0 = (double)__fmul_rn(__fsub_rn(np.b, np.a), 1.0f / 1024.0f);  // exact: power of two
     const double c[3] = {pq.x, pq.y, pq.z};
     bool ok = true;
 #pragma unroll

@@ -228,6 +228,16 @@ __global__ void k_morton_keys(const uint32_t* __restrict__ cell0, int n, uint32_
     idx[s] = s;
 }
 
+// Batched clouds: the cloud id above the Morton key keeps each cloud's rows together.
+__global__ void k_morton_keys64(const uint32_t* __restrict__ cell0, const uint16_t* __restrict__ cloud, int n,
+                                unsigned long long* __restrict__ key, int* __restrict__ idx) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t c = cell0[s];
+    key[s] = ((unsigned long long)cloud[s] << 30) | (spread3(c) | (spread3(c >> 10) << 1) | (spread3(c >> 20) << 2));
+    idx[s] = s;
+}
+
 __global__ void k_morton_rows(const int* __restrict__ perm, const int* __restrict__ off, int n, int* __restrict__ inv,
                               int* __restrict__ len) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -304,20 +314,35 @@ static egt_status morton_prepare(egt_handle* h) {
             EGT_CUDA_TRY(dev_alloc(h, &h->m_col, sizeof(int) * std::max<int64_t>(nnz, 1)));
             h->m_cap = std::max<int64_t>(nnz, 1);
         }
-        uint32_t *kin = nullptr, *kout = nullptr;
+        // keys: 30-bit Morton code of the level-0 cell, below the cloud id for batches
+        const bool wide = h->cloud_of != nullptr;
+        const int end_bit = wide ? 30 + h->cloud_bits : 30;
+        const size_t kb = wide ? sizeof(unsigned long long) : sizeof(uint32_t);
+        void *kin = nullptr, *kout = nullptr;
         int *idx = nullptr, *len = nullptr;
-        EGT_CUDA_TRY(cudaMallocAsync((void**)&kin, sizeof(uint32_t) * n, st));
-        EGT_CUDA_TRY(cudaMallocAsync((void**)&kout, sizeof(uint32_t) * n, st));
+        EGT_CUDA_TRY(cudaMallocAsync(&kin, kb * n, st));
+        EGT_CUDA_TRY(cudaMallocAsync(&kout, kb * n, st));
         EGT_CUDA_TRY(cudaMallocAsync((void**)&idx, sizeof(int) * n, st));
         EGT_CUDA_TRY(cudaMallocAsync((void**)&len, sizeof(int) * (n + 1), st));
-        k_morton_keys<<<G, 256, 0, st>>>(h->cell0, n, kin, idx);
+        if (wide) k_morton_keys64<<<G, 256, 0, st>>>(h->cell0, h->cloud_of, n, (unsigned long long*)kin, idx);
+        else k_morton_keys<<<G, 256, 0, st>>>(h->cell0, n, (uint32_t*)kin, idx);
         EGT_LAUNCH_CHECK();
         size_t t_sort = 0, t_scan = 0;
-        EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, t_sort, kin, kout, idx, h->m_perm, n, 0, 30, st));
+        if (wide)
+            EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, t_sort, (unsigned long long*)kin,
+                                                         (unsigned long long*)kout, idx, h->m_perm, n, 0, end_bit, st));
+        else
+            EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, t_sort, (uint32_t*)kin, (uint32_t*)kout, idx,
+                                                         h->m_perm, n, 0, end_bit, st));
         EGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, t_scan, len, h->m_off, n + 1, st));
         void* tmp = nullptr;
         EGT_TRY(scratch_reserve(h, std::max(t_sort, t_scan), &tmp));
-        EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, t_sort, kin, kout, idx, h->m_perm, n, 0, 30, st));
+        if (wide)
+            EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, t_sort, (unsigned long long*)kin,
+                                                         (unsigned long long*)kout, idx, h->m_perm, n, 0, end_bit, st));
+        else
+            EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, t_sort, (uint32_t*)kin, (uint32_t*)kout, idx,
+                                                         h->m_perm, n, 0, end_bit, st));
         k_morton_rows<<<G, 256, 0, st>>>(h->m_perm, h->csr_off, n, h->m_inv, len);
         EGT_LAUNCH_CHECK();
         EGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, t_scan, len, h->m_off, n + 1, st));
@@ -362,7 +387,8 @@ egt_status run_taubin(egt_handle* h, int iters, float lambda, float mu) {
         }
         const void* key[4] = {h->m_p, h->m_pb, h->t_uni, h->t_loc};
         const bool reuse = h->taubin_exec && h->taubin_iters == iters && h->taubin_lambda == lambda &&
-                           h->taubin_mu == mu && std::equal(key, key + 4, h->taubin_key);
+                           h->taubin_mu == mu && h->taubin_graph_mode == h->taubin_mode &&
+                           std::equal(key, key + 4, h->taubin_key);
         if (!reuse) {
             if (h->taubin_exec) { cudaGraphExecDestroy(h->taubin_exec); h->taubin_exec = nullptr; }
             // capture the 2*iters half-steps once; replays reuse the executable graph
@@ -373,8 +399,13 @@ egt_status run_taubin(egt_handle* h, int iters, float lambda, float mu) {
             cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
             if (e == cudaSuccess) {
                 for (int it = 0; it < iters && s == EGT_OK; it++) {
-                    s = staged_launch(h, h->m_p, h->m_pb, lambda, cap);
-                    if (s == EGT_OK) s = staged_launch(h, h->m_pb, h->m_p, mu, cap);
+                    if (h->taubin_mode == 0) {
+                        s = staged_launch(h, h->m_p, h->m_pb, lambda, cap);
+                        if (s == EGT_OK) s = staged_launch(h, h->m_pb, h->m_p, mu, cap);
+                    } else {  // direct gathers (no tile staging)
+                        s = taubin_launch(h->m_p, h->m_pb, h->m_off, h->m_col, n, lambda, cap);
+                        if (s == EGT_OK) s = taubin_launch(h->m_pb, h->m_p, h->m_off, h->m_col, n, mu, cap);
+                    }
                 }
                 cudaError_t e2 = cudaStreamEndCapture(cap, &g);
                 if (e2 != cudaSuccess && s == EGT_OK) { set_error(cuda_msg(e2, "EndCapture", __FILE__, __LINE__)); s = EGT_ERR_CUDA; }
@@ -394,6 +425,7 @@ egt_status run_taubin(egt_handle* h, int iters, float lambda, float mu) {
             cudaStreamDestroy(cap);
             EGT_TRY(s);
             h->taubin_iters = iters;
+            h->taubin_graph_mode = h->taubin_mode;
             h->taubin_lambda = lambda;
             h->taubin_mu = mu;
             std::copy(key, key + 4, h->taubin_key);
