@@ -57,6 +57,21 @@ def load_points(n=N_POINTS, seed=SEED):
     return xyz
 
 
+def profiled_traffic(kernel: str):
+    """DRAM bytes (read + write) per launch of `kernel` at the bench workload,
+    from the committed ncu summary (one capture of dram__bytes_read.sum and
+    dram__bytes_write.sum); None when no capture is recorded."""
+    import re
+    p = os.path.join(ROOT, "profiles", "dram_traffic_superquadrics_4m.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        m = re.match(r"\|\s*`" + re.escape(kernel) + r"`\s*\|.*\|\s*([0-9]+)\s*\|\s*$", line)
+        if m:
+            return int(m.group(1))
+    return None
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -281,9 +296,11 @@ def run_b200(args, world, rank, local):
             "taubin_roofline": {"bound": "hbm", "achieved": taubin_gbs, "peak": peak, "unit": "GB/s",
                                 "frac": taubin_gbs / peak, "peak_kind": peak_kind,
                                 "bytes_model": "2*iters*n*(28+4*m), m = kept neighbours per point",
-                                "m_mean": mbar},
+                                "m_mean": mbar, "traffic": profiled_traffic("k_taubin_staged"),
+                                "kernel": "k_taubin_staged (one half-step)"},
             "roofline": {"bound": "hbm", "achieved": knn_gbs, "peak": peak, "unit": "GB/s", "frac": knn_gbs / peak,
-                         "traffic": None, "kernel": "k_knn_plain", "peak_kind": peak_kind,
+                         "traffic": profiled_traffic("k_knn_plain"), "kernel": "k_knn_plain",
+                         "peak_kind": peak_kind,
                          "bytes_model": "n*(24+4k)"},
             "e2e": {"value": e2e_value, "unit": "Mqueries/s", "h2d_bytes_per_step": int(xyz.nbytes),
                     "d2h_bytes_per_step": int(n * K * 4)},

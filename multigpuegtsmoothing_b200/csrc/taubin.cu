@@ -16,9 +16,13 @@
 // of the level-0 cells: consecutive points then form compact 3-D blobs, so the
 // neighbours of a 256-row tile are few and mostly inside the tile; each
 // distinct neighbour position is gathered into shared memory once per tile and
-// the rows read them from there.  Relabelling changes neither a row's neighbour order nor any value, so
-// the result is the same bit for bit.
+// the rows read them from there.  Inside a tile the rows are then ordered by
+// decreasing neighbour count, so that the threads of a warp have equal work.
+// Relabelling changes neither a row's neighbour order nor any value, so the
+// result is the same bit for bit.  Each half-step is a programmatic dependent
+// launch: its prologue (CSR tables only) overlaps the previous half-step.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cub/cub.cuh>
 #include "egt_internal.cuh"
@@ -35,14 +39,21 @@ constexpr int kTileCap = 4608;   // CSR entries per staged tile (the 4M workload
 // fma(dz,dz, fma(dy,dy, dx*dx)), found by comparing candidate contractions
 // against the reference's own smoothed positions (0 mismatches on three
 // fixtures).
+//
+// The reference also forms q - p for the weighted sum.  Round-to-nearest
+// subtraction is antisymmetric, so q - p is exactly -(p - q) and the fused
+// multiply-adds below take the negated difference instead of a second
+// subtraction.  The one case where the two differ in sign bit -- a zero
+// difference -- gives w * (+-0) + c == c for every reachable c (the sums start
+// at +0 and never become -0), so the result is unchanged bit for bit.
 __device__ __forceinline__ void accumulate(float x1, float y1, float z1, float4 q, float& cx, float& cy,
                                            float& cz, float& sum) {
     const float dx = __fsub_rn(x1, q.x), dy = __fsub_rn(y1, q.y), dz = __fsub_rn(z1, q.z);
     const float distance = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
     const float w = expf(-distance);
-    cx = __fmaf_rn(w, __fsub_rn(q.x, x1), cx);
-    cy = __fmaf_rn(w, __fsub_rn(q.y, y1), cy);
-    cz = __fmaf_rn(w, __fsub_rn(q.z, z1), cz);
+    cx = __fmaf_rn(w, -dx, cx);
+    cy = __fmaf_rn(w, -dy, cy);
+    cz = __fmaf_rn(w, -dz, cz);
     sum = __fadd_rn(sum, w);
 }
 
@@ -86,49 +97,155 @@ __global__ void __launch_bounds__(256) k_taubin(const float4* __restrict__ pin, 
     pout[i] = row_update(pin, col, 0, __ldg(off + i), __ldg(off + i + 1), i, scale);
 }
 
-// Staged half-step.  For every kTile-row tile the distinct neighbour indices
-// (t_uni, precomputed once per CSR) are gathered into shared memory in one
-// parallel pass, and every CSR entry carries its 16-bit index into that list
-// (t_loc).  Rows then read their neighbours from shared memory in list order:
-// each distinct position is fetched from global memory once per tile instead
-// of once per reference.  Tiles whose lists would not fit (t_nu < 0) gather
-// from global memory directly.
-constexpr int kUCap = 1024;      // distinct neighbours staged per tile (16 KB; 99.8% of tiles fit)
-constexpr size_t kStagedSmem = kUCap * sizeof(float4) + kTileCap * sizeof(uint16_t);
+// Programmatic dependent launch (griddepcontrol): wait() blocks until the
+// preceding grid in the stream has completed and its writes are visible (it
+// returns at once when the kernel was not launched as a dependent);
+// launch_dependents() lets the next grid start its prologue on free SMs.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;"); }
 
-__global__ void __launch_bounds__(kTile, 6) k_taubin_staged(const float4* __restrict__ pin, float4* __restrict__ pout,
-                                                         const int* __restrict__ off, const int* __restrict__ col,
-                                                         const int* __restrict__ t_uni,
-                                                         const uint16_t* __restrict__ t_loc,
-                                                         const int* __restrict__ t_nu, int n, float scale) {
+constexpr int kUCap = 1024;      // distinct neighbours staged per tile (16 KB; 99.8% of tiles fit)
+constexpr int kUPer = kUCap / kTile;  // staged neighbours per thread
+constexpr size_t kStageBytes = kUCap * sizeof(float4) + kTileCap * sizeof(uint16_t);
+constexpr int kStages = 2;       // tile buffers per block: one being computed, one being filled
+constexpr size_t kPipeSmem = kStages * kStageBytes;
+static_assert(kTileCap % 8 == 0, "t_loc tiles are copied in 8-entry vectors");
+static_assert(kStageBytes % 16 == 0, "stage buffers stay 16-byte aligned");
+
+// First t_loc slot of tile t: its first CSR offset moved up by 8 slots per
+// preceding tile and rounded up to a multiple of 8 (16 bytes).  Consecutive
+// tiles never overlap: base(t+1) >= e_lo(t+1) + 8(t+1) > base(t) + cnt(t).
+__host__ __device__ __forceinline__ int64_t loc_base(int64_t e_lo, int64_t tile) {
+    return (e_lo + 8 * tile + 7) & ~int64_t(7);
+}
+// t_loc length for nnz entries over `tiles` tiles, including the last tile's
+// rounded-up vector.
+inline int64_t loc_slots(int64_t nnz, int64_t tiles) { return nnz + 8 * tiles + 16; }
+
+// 16-byte global -> shared copies that complete asynchronously (cp.async,
+// bypassing L1); commit() closes a group, wait<N>() waits until at most N of
+// the calling thread's groups are still in flight.
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// What a thread needs to know about one tile before its data arrive: the
+// tile's CSR range, its distinct-neighbour count, this thread's share of the
+// distinct-neighbour indices and this thread's row range.  Reads only the CSR
+// tables, which no half-step writes.
+struct TileRegs {
+    int e_lo, e_hi, nu, e0, e1;
+    int uni[kUPer];
+};
+
+__device__ __forceinline__ TileRegs tile_regs(const int* __restrict__ off, const int* __restrict__ t_uni,
+                                              const int* __restrict__ t_nu, int tile, int n) {
+    TileRegs r;
+    const int base = tile * kTile, last = min(base + kTile, n), i = base + (int)threadIdx.x;
+    r.e_lo = __ldg(off + base);
+    r.e_hi = __ldg(off + last);
+    r.nu = __ldg(t_nu + tile);
+    r.e0 = i < n ? __ldg(off + i) : 0;
+    r.e1 = i < n ? __ldg(off + i + 1) : 0;
+#pragma unroll
+    for (int u = 0; u < kUPer; u++) {
+        const int j = (int)threadIdx.x + u * kTile;
+        r.uni[u] = (r.nu >= 0 && j < r.nu) ? __ldg(t_uni + r.e_lo + j) : 0;
+    }
+    return r;
+}
+
+// Starts the copies of one tile into a stage buffer: the tile's 16-bit
+// neighbour slots (contiguous, 16-byte aligned) and its distinct neighbour
+// positions (one 16-byte gather each).  Always commits one group.
+__device__ __forceinline__ void tile_fetch(const TileRegs& r, const float4* __restrict__ pin,
+                                           const uint16_t* __restrict__ t_loc, int tile, unsigned char* stage) {
+    if (r.nu >= 0) {
+        float4* s_pos = reinterpret_cast<float4*>(stage);
+        uint16_t* s_loc = reinterpret_cast<uint16_t*>(stage + kUCap * sizeof(float4));
+        const uint16_t* src = t_loc + loc_base(r.e_lo, tile);
+        const int nvec = (r.e_hi - r.e_lo + 7) >> 3;
+        for (int v = (int)threadIdx.x; v < nvec; v += kTile) cp_async16(s_loc + 8 * v, src + 8 * v);
+#pragma unroll
+        for (int u = 0; u < kUPer; u++) {
+            const int j = (int)threadIdx.x + u * kTile;
+            if (j < r.nu) cp_async16(s_pos + j, pin + r.uni[u]);
+        }
+    }
+    cp_async_commit();
+}
+
+// Staged half-step, persistent and double-buffered.  Every kTile-row tile
+// has its distinct neighbour indices (t_uni, precomputed once per CSR) and,
+// per CSR entry, a 16-bit index into that list (t_loc).  Block b takes tiles
+// b, b + gridDim.x, ...; while it computes one tile from shared memory, the
+// copies of its next tile are in flight into the other buffer, and the
+// registers for the tile after that are being loaded.  Each distinct
+// neighbour position is fetched from global memory once per tile, and rows
+// read their neighbours from shared memory in list order.  Tiles whose lists
+// do not fit (t_nu < 0) gather from global memory directly.  Within a tile the
+// rows are ordered by decreasing neighbour count (see morton_prepare), so
+// the 32 rows of a warp walk rows of nearly equal length.
+__global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restrict__ pin, float4* __restrict__ pout,
+                                                        const int* __restrict__ off, const int* __restrict__ col,
+                                                        const int* __restrict__ t_uni,
+                                                        const uint16_t* __restrict__ t_loc,
+                                                        const int* __restrict__ t_nu, int n, int tiles, float scale) {
     extern __shared__ __align__(16) unsigned char smem[];
-    float4* s_pos = reinterpret_cast<float4*>(smem);
-    uint16_t* s_loc = reinterpret_cast<uint16_t*>(smem + kUCap * sizeof(float4));
-    const int base = blockIdx.x * kTile;
-    const int last = min(base + kTile, n);
-    const int e_lo = __ldg(off + base), e_hi = __ldg(off + last);
-    const int nu = __ldg(t_nu + blockIdx.x);
-    if (nu >= 0) {
-        for (int u = threadIdx.x; u < nu; u += kTile) s_pos[u] = __ldg(pin + __ldg(t_uni + e_lo + u));
-        for (int t = threadIdx.x; t < e_hi - e_lo; t += kTile) s_loc[t] = __ldg(t_loc + e_lo + t);
-    }
-    __syncthreads();
-    const int i = base + threadIdx.x;
-    if (i >= n) return;
-    if (nu < 0) {  // tile too large to stage: plain gathers
-        const float4 p = __ldg(pin + i);
-        float cx = 0.0f, cy = 0.0f, cz = 0.0f, sum = 0.0f;
-        for (int e = __ldg(off + i); e < __ldg(off + i + 1); e++)
-            accumulate(p.x, p.y, p.z, __ldg(pin + __ldg(col + e)), cx, cy, cz, sum);
-        pout[i] = finish(p, cx, cy, cz, sum, scale);
-        return;
-    }
-    const float4 p = __ldg(pin + i);
-    const int e0 = __ldg(off + i) - e_lo, e1 = __ldg(off + i + 1) - e_lo;
-    float cx = 0.0f, cy = 0.0f, cz = 0.0f, sum = 0.0f;
+    int tile = blockIdx.x;
+    if (tile >= tiles) return;
+    // Before grid_dependency_wait() only the CSR tables are read: under
+    // programmatic dependent launch this overlaps the previous half-step.
+    TileRegs cur = tile_regs(off, t_uni, t_nu, tile, n);
+    int next = tile + gridDim.x;
+    TileRegs nxt = next < tiles ? tile_regs(off, t_uni, t_nu, next, n) : cur;
+    grid_dependency_wait();  // the previous half-step's positions are complete
+    grid_dependents_launch();
+    tile_fetch(cur, pin, t_loc, tile, smem);
+    int i = tile * kTile + (int)threadIdx.x;
+    float4 p = i < n ? __ldg(pin + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int j = 0; tile < tiles; j++) {
+        unsigned char* stage = smem + (j & 1) * kStageBytes;
+        // the next tile's copies go to the buffer computed in the previous round
+        float4 p_next = p;
+        if (next < tiles) {
+            tile_fetch(nxt, pin, t_loc, next, smem + ((j + 1) & 1) * kStageBytes);
+            const int in = next * kTile + (int)threadIdx.x;
+            if (in < n) p_next = __ldg(pin + in);
+        } else {
+            cp_async_commit();  // keep one group per round
+        }
+        const int after = next + (int)gridDim.x;
+        const TileRegs nn = after < tiles ? tile_regs(off, t_uni, t_nu, after, n) : nxt;
+        cp_async_wait<1>();  // this thread's copies of the current tile have landed
+        __syncthreads();     // ... and everyone else's
+        if (i < n) {
+            float cx = 0.0f, cy = 0.0f, cz = 0.0f, sum = 0.0f;
+            if (cur.nu < 0) {  // tile too large to stage: plain gathers
+                for (int e = cur.e0; e < cur.e1; e++)
+                    accumulate(p.x, p.y, p.z, __ldg(pin + __ldg(col + e)), cx, cy, cz, sum);
+            } else {
+                const float4* s_pos = reinterpret_cast<const float4*>(stage);
+                const uint16_t* s_loc = reinterpret_cast<const uint16_t*>(stage + kUCap * sizeof(float4));
+                const int e0 = cur.e0 - cur.e_lo, e1 = cur.e1 - cur.e_lo;
 #pragma unroll 4
-    for (int e = e0; e < e1; e++) accumulate(p.x, p.y, p.z, s_pos[s_loc[e]], cx, cy, cz, sum);
-    pout[i] = finish(p, cx, cy, cz, sum, scale);
+                for (int e = e0; e < e1; e++) accumulate(p.x, p.y, p.z, s_pos[s_loc[e]], cx, cy, cz, sum);
+            }
+            pout[i] = finish(p, cx, cy, cz, sum, scale);
+        }
+        __syncthreads();  // the buffer is free for the tile after next
+        tile = next;
+        next = after;
+        cur = nxt;
+        nxt = nn;
+        p = p_next;
+        i = tile * kTile + (int)threadIdx.x;
+    }
+    cp_async_wait<0>();
 }
 
 // Builds t_uni / t_loc / t_nu for one tile: block radix sort of the tile's
@@ -196,7 +313,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restr
             if (sm.uniq[mid] < v) lo = mid + 1;
             else hi = mid;
         }
-        t_loc[e_lo + i] = (uint16_t)lo;
+        t_loc[loc_base(e_lo, blockIdx.x) + i] = (uint16_t)lo;
     }
     if (threadIdx.x == 0) t_nu[blockIdx.x] = nu;
 }
@@ -236,6 +353,19 @@ __global__ void k_morton_keys64(const uint32_t* __restrict__ cell0, const uint16
     const uint32_t c = cell0[s];
     key[s] = ((unsigned long long)cloud[s] << 30) | (spread3(c) | (spread3(c >> 10) << 1) | (spread3(c >> 20) << 2));
     idx[s] = s;
+}
+
+// Sort keys that order the rows of every kTile-row tile of the Morton order
+// by decreasing neighbour count; a stable sort keeps equal counts in Morton
+// order.
+__global__ void k_degree_keys(const int* __restrict__ perm, const int* __restrict__ off, int n,
+                              uint32_t* __restrict__ key, int* __restrict__ val) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s = perm[i];
+    const int len = min(off[s + 1] - off[s], 255);
+    key[i] = ((uint32_t)(i / kTile) << 8) | (uint32_t)(255 - len);
+    val[i] = s;
 }
 
 __global__ void k_morton_rows(const int* __restrict__ perm, const int* __restrict__ off, int n, int* __restrict__ inv,
@@ -284,10 +414,26 @@ egt_status taubin_launch(const float4* pin, float4* pout, const int* off, const 
     return EGT_OK;
 }
 
-static egt_status staged_launch(egt_handle* h, const float4* pin, float4* pout, float scale, cudaStream_t st) {
+// One staged half-step: a persistent grid of at most one resident wave,
+// launched as a programmatic dependent of the previous kernel in the stream
+// (see k_taubin_tiles).
+static egt_status staged_launch(egt_handle* h, const float4* pin, float4* pout, float scale, unsigned blocks,
+                                cudaStream_t st) {
     const int n = (int)h->n;
-    k_taubin_staged<<<(unsigned)((n + kTile - 1) / kTile), kTile, kStagedSmem, st>>>(
-        pin, pout, h->m_off, h->m_col, h->t_uni, h->t_loc, h->t_nu, n, scale);
+    const int tiles = (n + kTile - 1) / kTile;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(std::min<unsigned>(blocks, (unsigned)tiles));
+    cfg.blockDim = dim3(kTile);
+    cfg.dynamicSmemBytes = kPipeSmem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    EGT_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_taubin_tiles, pin, pout, (const int*)h->m_off, (const int*)h->m_col,
+                                    (const int*)h->t_uni, (const uint16_t*)h->t_loc, (const int*)h->t_nu, n, tiles,
+                                    scale));
     EGT_LAUNCH_CHECK();
     return EGT_OK;
 }
@@ -335,29 +481,39 @@ static egt_status morton_prepare(egt_handle* h) {
             EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, t_sort, (uint32_t*)kin, (uint32_t*)kout, idx,
                                                          h->m_perm, n, 0, end_bit, st));
         EGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, t_scan, len, h->m_off, n + 1, st));
+        const int64_t tiles = (n + kTile - 1) / kTile;
+        int tile_bits = 0;
+        while ((int64_t(1) << tile_bits) < tiles) tile_bits++;
+        size_t t_deg = 0;
+        EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, t_deg, (uint32_t*)kin, (uint32_t*)kout, idx, h->m_perm,
+                                                     n, 0, 8 + tile_bits, st));
         void* tmp = nullptr;
-        EGT_TRY(scratch_reserve(h, std::max(t_sort, t_scan), &tmp));
+        EGT_TRY(scratch_reserve(h, std::max(std::max(t_sort, t_scan), t_deg), &tmp));
         if (wide)
             EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, t_sort, (unsigned long long*)kin,
                                                          (unsigned long long*)kout, idx, h->m_perm, n, 0, end_bit, st));
         else
             EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, t_sort, (uint32_t*)kin, (uint32_t*)kout, idx,
                                                          h->m_perm, n, 0, end_bit, st));
+        // within each tile, rows by decreasing neighbour count
+        k_degree_keys<<<G, 256, 0, st>>>(h->m_perm, h->csr_off, n, (uint32_t*)kin, idx);
+        EGT_LAUNCH_CHECK();
+        EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, t_deg, (uint32_t*)kin, (uint32_t*)kout, idx, h->m_perm, n,
+                                                     0, 8 + tile_bits, st));
         k_morton_rows<<<G, 256, 0, st>>>(h->m_perm, h->csr_off, n, h->m_inv, len);
         EGT_LAUNCH_CHECK();
         EGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, t_scan, len, h->m_off, n + 1, st));
         k_morton_cols<<<G, 256, 0, st>>>(h->m_perm, h->m_inv, h->csr_off, h->csr_col, h->m_off, n, h->m_col);
         EGT_LAUNCH_CHECK();
         // per-tile distinct-neighbour lists for the staged half-step
-        const unsigned tiles = (unsigned)((n + kTile - 1) / kTile);
         if (h->t_uni) dev_free(h, h->t_uni);
         if (h->t_loc) dev_free(h, h->t_loc);
         if (h->t_nu) dev_free(h, h->t_nu);
         h->t_uni = nullptr; h->t_loc = nullptr; h->t_nu = nullptr;
         EGT_CUDA_TRY(dev_alloc(h, &h->t_uni, sizeof(int) * std::max<int64_t>(nnz, 1)));
-        EGT_CUDA_TRY(dev_alloc(h, &h->t_loc, sizeof(uint16_t) * std::max<int64_t>(nnz, 1)));
+        EGT_CUDA_TRY(dev_alloc(h, &h->t_loc, sizeof(uint16_t) * loc_slots(nnz, tiles)));
         EGT_CUDA_TRY(dev_alloc(h, &h->t_nu, sizeof(int) * tiles));
-        k_tile_build<<<tiles, kBuildThreads, 0, st>>>(h->m_off, h->m_col, n, h->t_uni, h->t_loc, h->t_nu);
+        k_tile_build<<<(unsigned)tiles, kBuildThreads, 0, st>>>(h->m_off, h->m_col, n, h->t_uni, h->t_loc, h->t_nu);
         EGT_LAUNCH_CHECK();
         cudaFreeAsync(kin, st);
         cudaFreeAsync(kout, st);
@@ -379,12 +535,26 @@ egt_status run_taubin(egt_handle* h, int iters, float lambda, float mu) {
     EGT_CUDA_TRY(cudaEventRecord(h->ev[6], st));
     if (iters > 0) {
         EGT_TRY(morton_prepare(h));
-        static bool smem_set = false;
-        if (!smem_set) {
-            EGT_CUDA_TRY(cudaFuncSetAttribute(k_taubin_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)kStagedSmem));
-            smem_set = true;
+        // function attributes are per device: set them once on each, and size
+        // the persistent grid from the occupancy they allow
+        static std::atomic<uint64_t> attr_set{0};
+        static std::atomic<unsigned> wave[64];
+        int dev = 0;
+        EGT_CUDA_TRY(cudaGetDevice(&dev));
+        if (!(attr_set.load() >> (dev & 63) & 1)) {
+            EGT_CUDA_TRY(cudaFuncSetAttribute(k_taubin_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)kPipeSmem));
+            // the whole unified L1/shared array as shared memory, so that four
+            // 50-KB blocks fit on an SM
+            EGT_CUDA_TRY(cudaFuncSetAttribute(k_taubin_tiles, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                              (int)cudaSharedmemCarveoutMaxShared));
+            int sms = 0, per = 0;
+            EGT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            EGT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_taubin_tiles, kTile, kPipeSmem));
+            wave[dev & 63].store((unsigned)std::max(1, sms * std::max(per, 1)));
+            attr_set.fetch_or(uint64_t(1) << (dev & 63));
         }
+        const unsigned blocks = wave[dev & 63].load();
         const void* key[4] = {h->m_p, h->m_pb, h->t_uni, h->t_loc};
         const bool reuse = h->taubin_exec && h->taubin_iters == iters && h->taubin_lambda == lambda &&
                            h->taubin_mu == mu && h->taubin_graph_mode == h->taubin_mode &&
@@ -400,8 +570,8 @@ egt_status run_taubin(egt_handle* h, int iters, float lambda, float mu) {
             if (e == cudaSuccess) {
                 for (int it = 0; it < iters && s == EGT_OK; it++) {
                     if (h->taubin_mode == 0) {
-                        s = staged_launch(h, h->m_p, h->m_pb, lambda, cap);
-                        if (s == EGT_OK) s = staged_launch(h, h->m_pb, h->m_p, mu, cap);
+                        s = staged_launch(h, h->m_p, h->m_pb, lambda, blocks, cap);
+                        if (s == EGT_OK) s = staged_launch(h, h->m_pb, h->m_p, mu, blocks, cap);
                     } else {  // direct gathers (no tile staging)
                         s = taubin_launch(h->m_p, h->m_pb, h->m_off, h->m_col, n, lambda, cap);
                         if (s == EGT_OK) s = taubin_launch(h->m_pb, h->m_p, h->m_off, h->m_col, n, mu, cap);
