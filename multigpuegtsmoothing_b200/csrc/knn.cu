@@ -24,6 +24,7 @@
 // list (the dedup rule rejects it) or farther than the k-th distance of that
 // time, which never grows (the admission rule rejects it), so offering it again
 // cannot change the list.
+#include <atomic>
 #include <map>
 #include <mutex>
 
@@ -39,7 +40,7 @@ namespace {
 // a time, so that a warp that drew cheap queries moves on instead of idling
 // until the most expensive query of its block is done.
 template <int S, bool kFast>
-__global__ void __launch_bounds__(kWarps * 32) k_knn_plain(KnnArgs a) {
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_plain(KnnArgs a) {
     __shared__ int s_pref[kWarps][32];
     __shared__ int s_start[kWarps][32];
     __shared__ float s_md[kWarps][32 * S];
@@ -67,9 +68,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_knn_plain(KnnArgs a) {
 
 // ---------------------------------------------------------------------------
 // Proposal-driven search (an extension of this project).  The query's box
-// (class from the proposal network) is streamed row by row, nearest rows
-// first, keeping the k+1 smallest distances.  The result is accepted only when
-// it provably equals the plain search's list:
+// (class from the proposal network) is searched for its k+1 smallest
+// distances.  The result is accepted only when it provably equals the plain
+// search's list:
 //   (1) >= k candidates and the k+1 smallest distances pairwise distinct, so
 //       the sorted list does not depend on the candidate order;
 //   (2) the ball of radius sqrt(kth) + margin lies inside the searched box,
@@ -83,56 +84,225 @@ __global__ void __launch_bounds__(kWarps * 32) k_knn_plain(KnnArgs a) {
 //       of G must be visited by step sf;
 //   (4) no cell of the levels visited up to sf holds >= max_points_in_cell
 //       points (the plain search would have invalidated the query).
-// The box may be cut short after any complete ring of rows whose sub-box
-// already passes (2).  A failed check runs the plain search for the query.
+// The box's candidates below its cut are collected and the k+1 smallest
+// selected once (select_list).  A failed check, or a box whose candidates do
+// not fit the collection buffer, runs the plain search for the query.
 
-// Streams the points of m row ranges (range l held by lane l as [cs, ce))
-// through the list, admitting only distances below `cut` as well.
+// Streams the points of m row ranges (range l held by lane l as [cs, ce)),
+// software-pipelined as in stream_cells, through the list, admitting only
+// distances below `cut` as well.
 template <int S>
 __device__ __forceinline__ void stream_ranges(WarpList<S>& L, int m, int cs, int ce, const int* __restrict__ order,
                                               const float4* __restrict__ p4, int q, float4 pq, float thres, float cut,
                                               int lane, int* s_pref, int* s_start, float* s_md, int* s_mp) {
-    int incl = lane < m ? ce - cs : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    __syncwarp();
-    s_pref[lane] = incl;
-    s_start[lane] = cs;
-    __syncwarp();
-    for (int base = 0; base < total; base += 32) {
-        const int j = base + lane;
+    const RangeSeq seq = range_seq(lane < m ? ce - cs : 0, cs, lane, s_pref, s_start);
+    int pA = seq_index(seq, 32, lane, order);
+    int pB = seq_index(seq, 0, lane, order);
+    float4 vB = stream_point(pB, q, p4);
+    for (int base = 0; base < seq.total; base += 32) {
+        const int p = pB;
+        const float4 v = vB;
+        pB = pA;
+        vB = stream_point(pB, q, p4);
+        pA = seq_index(seq, base + 64, lane, order);
         float d = 1e30f;
-        int p = -1;
         bool ok = false;
-        if (j < total) {
-            int lo = 0, hi = m - 1;  // first range with incl > j
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (s_pref[mid] > j) hi = mid;
-                else lo = mid + 1;
-            }
-            const int excl = lo > 0 ? s_pref[lo - 1] : 0;
-            const int pos = s_start[lo] + (j - excl);
-            p = order ? order[pos] : pos;
-            if (p != q) {
-                const float4 v = p4[p];
-                d = fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z);
-                ok = d <= thres;
-            }
+        if (p >= 0 && p != q) {
+            d = fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z);
+            ok = d <= thres;
         }
         offer<false, S>(L, d, p, ok && d < L.kth && d < cut, lane, s_md, s_mp);
     }
+}
+
+// For lists of more than 64 slots the box candidates are not merged into the
+// list as they stream: every candidate below the box's cut is collected into
+// a per-warp buffer, and the k+1 smallest are selected once at the end
+// (select_list).  Merging costs grow with the list; selection costs do not
+// (measured on the 20M-point k=64 sheets: 153 ms merged, 107 ms collected;
+// on the 4M-point k=40 superquadrics merging stays ahead, 19.4 ms against
+// 20.6 ms).  Per-warp scratch of the proposal-driven kernel, in dynamic
+// shared memory.
+constexpr int kCollectCap = 448;  // candidates collected per box (more: the query runs the plain search)
+constexpr int kSelectCap = 128;   // selected candidates plus the boundary bucket
+constexpr int kBuckets = 256;
+struct BoxScratch {
+    float* cd;   // [kCollectCap] collected distances
+    int* cp;     // [kCollectCap] collected points
+    int* hist;   // [kBuckets]
+    float* sd;   // [kSelectCap] selected candidates in bucket order
+    int* sp;
+};
+constexpr size_t kBoxScratchBytes = (size_t)kCollectCap * 8 + kBuckets * 4 + kSelectCap * 8;
+
+__device__ __forceinline__ BoxScratch box_scratch(unsigned char* base, int warp) {
+    unsigned char* w = base + (size_t)warp * kBoxScratchBytes;
+    BoxScratch b;
+    b.cd = reinterpret_cast<float*>(w);
+    b.cp = reinterpret_cast<int*>(w + kCollectCap * 4);
+    b.hist = reinterpret_cast<int*>(w + kCollectCap * 8);
+    b.sd = reinterpret_cast<float*>(w + kCollectCap * 8 + kBuckets * 4);
+    b.sp = reinterpret_cast<int*>(w + kCollectCap * 8 + kBuckets * 4 + kSelectCap * 4);
+    return b;
+}
+
+// Streams the points of m row ranges (range l held by lane l as [cs, ce)),
+// software-pipelined as in stream_cells, collecting every candidate with
+// d <= thres and d < cut.  Returns the new collected count
+// (uniform; it may exceed kCollectCap, in which case the excess is dropped and
+// the caller gives up).  dmax: the lane's largest collected distance.
+__device__ __forceinline__ int stream_collect(int m, int cs, int ce, const int* __restrict__ order,
+                                              const float4* __restrict__ p4, int q, float4 pq, float thres, float cut,
+                                              int lane, int* s_pref, int* s_start, const BoxScratch& bx, int count,
+                                              float& dmax) {
+    const RangeSeq seq = range_seq(lane < m ? ce - cs : 0, cs, lane, s_pref, s_start);
+    int pA = seq_index(seq, 32, lane, order);
+    int pB = seq_index(seq, 0, lane, order);
+    float4 vB = stream_point(pB, q, p4);
+    for (int base = 0; base < seq.total; base += 32) {
+        const int p = pB;
+        const float4 v = vB;
+        pB = pA;
+        vB = stream_point(pB, q, p4);
+        pA = seq_index(seq, base + 64, lane, order);
+        float d = 0.0f;
+        bool ok = false;
+        if (p >= 0 && p != q) {
+            d = fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z);
+            ok = d <= thres && d < cut;
+        }
+        const unsigned mk = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+            const int at = count + __popc(mk & ((1u << lane) - 1u));
+            if (at < kCollectCap) { bx.cd[at] = d; bx.cp[at] = p; }
+            dmax = fmaxf(dmax, d);
+        }
+        count += __popc(mk);
+    }
+    return count;
+}
+
+// (r - margin)^2 rounded down, r = the query's distance to the nearest
+// in-grid face of the box sub-box of y/z half-width `ring` (0 when r <= margin;
+// 3e38 when no face is inside the grid).  A squared distance below it gives a
+// ball that passes ball_in_box for that sub-box.
+__device__ __forceinline__ float ring_inner_sq(const NormParams& np, float4 pq, int cls, int ring, uint32_t c0) {
+    int lo[3], end[3];
+    box_bounds(cls, ring, c0, lo, end);
+    const double h0 = (double)__fmul_rn(__fsub_rn(np.b, np.a), 1.0f / 1024.0f);
+    const double c[3] = {pq.x, pq.y, pq.z};
+    double fnear = 1e30;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        if (lo[d] > 0) fnear = fmin(fnear, c[d] - ((double)np.a + lo[d] * h0));
+        if (end[d] < 1024) fnear = fmin(fnear, ((double)np.a + end[d] * h0) - c[d]);
+    }
+    if (fnear >= 1e29) return 3.0e38f;
+    const double t = fnear - kBoxMargin;
+    return t > 0.0 ? __double2float_rd(t * t) : 0.0f;
+}
+
+// Bucket of a collected distance: 256 buckets, linear in d over [0, dmax]
+// (monotone in d, so bucket order never contradicts distance order).
+__device__ __forceinline__ int dist_bucket(float d, float scale) {
+    return min((int)__fmul_rn(d, scale), kBuckets - 1);
+}
+
+// Puts the `need` smallest of the `count` collected candidates, ordered by
+// (distance, index), into slots [0, need) of L (need <= L.k).  A counting
+// pass over 256 distance buckets finds the bucket holding the need-th
+// smallest; the candidates of that and lower buckets are placed in bucket
+// order and ranked inside their bucket.  Returns false when those candidates
+// do not fit in the selection buffer.
+template <int S>
+__device__ bool select_list(WarpList<S>& L, const BoxScratch& bx, int count, int need, float dmax, float* md,
+                            int* mp, int lane) {
+    const float scale = dmax > 0.0f ? __fdiv_rn(255.99f, dmax) : 0.0f;
+#pragma unroll
+    for (int i = 0; i < kBuckets / 32; i++) bx.hist[lane + 32 * i] = 0;
+    __syncwarp();
+    for (int e = lane; e < count; e += 32) atomicAdd(&bx.hist[dist_bucket(bx.cd[e], scale)], 1);
+    __syncwarp();
+    // lane l owns buckets [8l, 8l+8)
+    int c8[kBuckets / 32], sum = 0;
+#pragma unroll
+    for (int i = 0; i < kBuckets / 32; i++) { c8[i] = bx.hist[lane * (kBuckets / 32) + i]; sum += c8[i]; }
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int excl = incl - sum;
+    const int target = need - 1;  // rank of the last selected candidate
+    const int wl = __ffs(__ballot_sync(0xffffffffu, excl <= target && target < incl)) - 1;
+    int bstar = 0, below = 0;
+    if (lane == wl) {
+        int acc = excl;
+#pragma unroll
+        for (int i = 0; i < kBuckets / 32; i++) {
+            if (acc + c8[i] > target) { bstar = lane * (kBuckets / 32) + i; below = acc; break; }
+            acc += c8[i];
+        }
+    }
+    bstar = __shfl_sync(0xffffffffu, bstar, wl);
+    below = __shfl_sync(0xffffffffu, below, wl);
+    const int tot = below + bx.hist[bstar];
+    __syncwarp();
+    if (tot > kSelectCap) return false;
+    // bucket starts (exclusive prefix) for the buckets that take part
+    {
+        int run = excl;
+#pragma unroll
+        for (int i = 0; i < kBuckets / 32; i++) {
+            const int b = lane * (kBuckets / 32) + i;
+            if (b <= bstar) bx.hist[b] = run;
+            run += c8[i];
+        }
+    }
+    __syncwarp();
+    for (int e = lane; e < count; e += 32) {
+        const float d = bx.cd[e];
+        const int b = dist_bucket(d, scale);
+        if (b <= bstar) {
+            const int slot = atomicAdd(&bx.hist[b], 1);
+            bx.sd[slot] = d;
+            bx.sp[slot] = bx.cp[e];
+        }
+    }
+    __syncwarp();
+    // hist[b] is now the end of bucket b, and the start of bucket b+1
+    for (int i = lane; i < tot; i += 32) {
+        const float d = bx.sd[i];
+        const int p = bx.sp[i];
+        const int b = dist_bucket(d, scale);
+        int r = b > 0 ? bx.hist[b - 1] : 0;
+        const int e1 = bx.hist[b];
+        for (int j = r; j < e1; j++) {
+            const float dj = bx.sd[j];
+            r += (dj < d || (dj == d && bx.sp[j] < p)) ? 1 : 0;
+        }
+        if (r < need) { md[r] = d; mp[r] = p; }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        L.dist[s] = t < need ? md[t] : 1e10f;
+        L.idx[s] = t < need ? mp[t] : -1;
+    }
+    __syncwarp();
+    L.counter = need;
+    L.kth = L.fetch_dist(L.k - 1);
+    return true;
 }
 
 // Box search + certification.  Returns true with L holding the plain
 // search's list in slots [0, k) and `reached` its level.
 template <int S>
 __device__ bool box_search(const KnnArgs& a, const NormParams& np, int q, float4 pq, int cls, WarpList<S>& L,
-                           int lane, int* s_pref, int* s_start, float* s_md, int* s_mp, int& reached) {
+                           int lane, int* s_pref, int* s_start, float* s_md, int* s_mp, const BoxScratch& bx,
+                           int& reached) {
     const int lvl = kBoxClass[cls][0], R = kBoxClass[cls][1];
     const LevelDev& LV = a.lv[lvl];
     const uint32_t c0 = __float_as_uint(pq.w);
@@ -158,28 +328,63 @@ __device__ bool box_search(const KnnArgs& a, const NormParams& np, int q, float4
         if (fnear < 1e29) cut = __double2float_ru(fmax(fnear, 0.0) * fmax(fnear, 0.0));
     }
     const int nrows = (2 * R + 1) * (2 * R + 1);
-    int ring = -1;
-    bool inside = false;
-    for (int rb = 0; rb < nrows && !inside; rb += 32) {
+    constexpr bool kCollect = S > 2;
+    int count = 0, ring = -1;
+    float dmax = 0.0f;
+    bool enough = false;
+    // Rows are streamed 32 per round, ring by ring.  After a round that
+    // completes a ring: once k candidate distances lie
+    // below its sub-box's inner radius (less the margin), squared, the k
+    // nearest points of the cloud -- and every point as near as the k-th --
+    // have been streamed, and the rest of the box cannot change the list up
+    // to its k-th slot or the tie check there.
+    for (int rb = 0; rb < nrows && !enough;) {
+        const int re = min(rb + 32, nrows);
         int2 rg = make_int2(0, 0);
         const int t = rb + lane;
-        if (t < nrows) rg = row_points(LV, cix - R, cix + R, ciy + kRowOrder[t][0], ciz + kRowOrder[t][1]);
-        stream_ranges<S>(L, min(32, nrows - rb), rg.x, rg.y, lvl ? LV.order : nullptr, a.p4, q, pq, np.thres, cut,
-                         lane, s_pref, s_start, s_md, s_mp);
-        // largest ring of rows completely streamed
-        const int done = min(rb + 32, nrows);
+        if (t < re) rg = row_points(LV, cix - R, cix + R, ciy + kRowOrder[t][0], ciz + kRowOrder[t][1]);
+        const int* order = lvl ? LV.order : nullptr;
+        if constexpr (kCollect) {
+            count = stream_collect(re - rb, rg.x, rg.y, order, a.p4, q, pq, np.thres, cut, lane, s_pref, s_start,
+                                   bx, count, dmax);
+            if (count > kCollectCap) return false;
+        } else {
+            stream_ranges<S>(L, re - rb, rg.x, rg.y, order, a.p4, q, pq, np.thres, cut, lane, s_pref, s_start, s_md,
+                             s_mp);
+        }
+        rb = re;
         int j = ring;
-        while ((2 * j + 3) * (2 * j + 3) <= done) j++;
+        while ((2 * j + 3) * (2 * j + 3) <= rb) j++;
         if (j > ring) {
             ring = j;
-            if (L.counter >= k) {
-                int lo[3], end[3];
-                box_bounds(cls, ring, c0, lo, end);
-                inside = ball_in_box(np, pq, L.fetch_dist(k - 1), lo, end);  // (2)
+            if (ring < R) {
+                const float inner = ring_inner_sq(np, pq, cls, ring, c0);
+                if constexpr (kCollect) {
+                    if (count >= k) {
+                        int below = 0;
+                        for (int e = lane; e < count; e += 32) below += bx.cd[e] < inner ? 1 : 0;
+                        enough = __reduce_add_sync(0xffffffffu, below) >= k;
+                    }
+                } else {
+                    enough = L.counter >= k && L.fetch_dist(k - 1) < inner;
+                }
             }
         }
     }
-    if (!inside) return false;
+    if constexpr (kCollect) {
+        if (count < k) return false;
+        dmax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(dmax)));  // d >= 0: bit order
+        if (!select_list<S>(L, bx, count, min(count, k + 1), dmax, s_md, s_mp, lane)) return false;
+    } else if (L.counter < k) {
+        return false;
+    }
+    // (2) the k-th ball lies inside the searched box (the sub-box of `ring`
+    // when the search stopped early)
+    {
+        int lo[3], end[3];
+        box_bounds(cls, enough ? ring : R, c0, lo, end);
+        if (!ball_in_box(np, pq, L.fetch_dist(k - 1), lo, end)) return false;
+    }
     // (1) the kept distances are strictly increasing
     if (has_ties(L, min(L.counter, k + 1), lane)) return false;
     const float kth = L.fetch_dist(k - 1);
@@ -224,6 +429,7 @@ __device__ bool box_search(const KnnArgs& a, const NormParams& np, int q, float4
 
 template <int S>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_learned(KnnArgs a, const uint8_t* __restrict__ cls) {
+    extern __shared__ __align__(16) unsigned char s_scratch[];  // kWarps * kBoxScratchBytes
     __shared__ int s_pref[kWarps][32];
     __shared__ int s_start[kWarps][32];
     __shared__ float s_md[kWarps][32 * S];
@@ -242,7 +448,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_learned(KnnArgs
             int reached = 0;
             const int c = cls[q];
             if (c < kPropPlain) {
-                ok = box_search<S>(a, np, q, pq, c, L, lane, s_pref[w], s_start[w], s_md[w], s_mp[w], reached);
+                ok = box_search<S>(a, np, q, pq, c, L, lane, s_pref[w], s_start[w], s_md[w], s_mp[w],
+                                   box_scratch(s_scratch, w), reached);
                 if (lane == 0) {
                     atomicAdd(&s_box, 1u);
                     if (ok) atomicAdd(&s_cert, 1u);
@@ -267,7 +474,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_learned(KnnArgs
 
 // Blocks of one resident wave of a persistent kernel, per (kernel, device).
 template <typename K>
-egt_status wave_blocks(K kernel, int64_t n, unsigned* out) {
+egt_status wave_blocks(K kernel, int64_t n, unsigned* out, size_t dyn_smem = 0) {
     static std::mutex mu;
     static std::map<std::pair<const void*, int>, int> cache;
     int dev = 0;
@@ -282,7 +489,7 @@ egt_status wave_blocks(K kernel, int64_t n, unsigned* out) {
     if (!blocks) {
         int sms = 0, per = 0;
         EGT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        EGT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kWarps * 32, 0));
+        EGT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kWarps * 32, dyn_smem));
         blocks = std::max(1, sms * std::max(per, 1));
         std::lock_guard<std::mutex> lock(mu);
         cache[key] = blocks;
@@ -294,9 +501,17 @@ egt_status wave_blocks(K kernel, int64_t n, unsigned* out) {
 
 template <int S>
 egt_status launch_learned(const KnnArgs& a, const uint8_t* cls, cudaStream_t st) {
+    constexpr size_t smem = S > 2 ? kWarps * kBoxScratchBytes : 0;  // collection buffers (box_search)
+    static std::atomic<uint64_t> attr_set{0};  // per device
+    int dev = 0;
+    EGT_CUDA_TRY(cudaGetDevice(&dev));
+    if (smem && !(attr_set.load() >> (dev & 63) & 1)) {
+        EGT_CUDA_TRY(cudaFuncSetAttribute(k_knn_learned<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set.fetch_or(uint64_t(1) << (dev & 63));
+    }
     unsigned G = 0;
-    EGT_TRY(wave_blocks(k_knn_learned<S>, a.n, &G));
-    k_knn_learned<S><<<G, kWarps * 32, 0, st>>>(a, cls);
+    EGT_TRY(wave_blocks(k_knn_learned<S>, a.n, &G, smem));
+    k_knn_learned<S><<<G, kWarps * 32, smem, st>>>(a, cls);
     EGT_LAUNCH_CHECK();
     return EGT_OK;
 }

@@ -219,6 +219,59 @@ __device__ __forceinline__ void merge_batch(WarpList<S>& L, float d, int p, bool
     L.kth = L.fetch_dist(cap - 1);
 }
 
+// Merges a small batch of admitted candidates (ok; `mask` = their lanes)
+// into the sorted list without sorting the batch: each candidate's slot is
+// the number of list elements <= its distance (one binary search per lane)
+// plus the number of candidates ordered before it (distance, then lane); each
+// list element moves down by the number of candidates below it.  Equal
+// distances place the list's element first and candidates in lane order, as
+// merge_batch does up to the order of equal batch elements, which only the
+// tie-free candidate streams of merge_batch reach.  Cost: one binary search
+// plus a few instructions per candidate, against a full 32-wide sort.
+template <int S>
+__device__ __forceinline__ void merge_rank(WarpList<S>& L, float d, int p, bool ok, unsigned mask, int lane,
+                                           float* sd, int* sp) {
+    constexpr int kSteps = S <= 1 ? 6 : S <= 2 ? 7 : S <= 4 ? 8 : 9;  // > log2(32*S)
+    const int cnt = L.counter, cap = L.k;
+    int lo = 0, hi = cnt;  // list elements <= d
+#pragma unroll
+    for (int it = 0; it < kSteps; it++) {
+        const int mid = (lo + hi) >> 1;
+        const float v = list_dist_at(L, mid);
+        if (lo < hi) {
+            if (v <= d) lo = mid + 1;
+            else hi = mid;
+        }
+    }
+    int rank = lo;
+    int sh[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) sh[s] = 0;
+    for (unsigned m = mask; m; m &= m - 1) {
+        const int src = __ffs(m) - 1;
+        const float dj = __shfl_sync(0xffffffffu, d, src);
+        rank += (dj < d || (dj == d && src < lane)) ? 1 : 0;
+#pragma unroll
+        for (int s = 0; s < S; s++) sh[s] += dj < L.dist[s] ? 1 : 0;
+    }
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s, r = t + sh[s];
+        if (t < cnt && r < cap) { sd[r] = L.dist[s]; sp[r] = L.idx[s]; }
+    }
+    if (ok && rank < cap) { sd[rank] = d; sp[rank] = p; }
+    __syncwarp();
+    const int nc = min(cnt + __popc(mask), cap);
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        if (t < nc) { L.dist[s] = sd[t]; L.idx[s] = sp[t]; }
+    }
+    __syncwarp();
+    L.counter = nc;
+    L.kth = L.fetch_dist(cap - 1);
+}
+
 // Locate cell (cx,cy,cz) of a level: returns [start,end) into the level's
 // order array, or start == end == -1 when the cell is empty / out of range.
 __device__ __forceinline__ int2 find_cell(const LevelDev& L, int cx, int cy, int cz) {

@@ -2,6 +2,7 @@
 // (knn.cu) and the batched kernels (batch.cu).  See knn.cu for the reference
 // correspondence and the design.
 #pragma once
+#include <climits>
 #include "egt_internal.cuh"
 #include "knn_common.cuh"
 
@@ -22,7 +23,8 @@ struct KnnArgs {
 
 constexpr int kWarps = 8;
 // The search kernels are latency-bound: keep four blocks (32 warps) resident
-// per SM, which caps them at 64 registers.
+// per SM, which caps them at 64 registers (measured faster than fewer,
+// larger-register blocks for lists of up to 96 slots).
 constexpr int kMinBlocks = 4;
 
 // Continue decision after the last cube of a shell (GridKNNCuda.cu:694-741).
@@ -53,11 +55,20 @@ __device__ __forceinline__ bool decide(const NormParams& np, int L, int o, int c
     return more;
 }
 
-// Batches admitting at least this many candidates are merged in one step.
+// Batches admitting at least kMergeMin candidates are merged in one step:
+// for lists of up to 64 slots by ranks (merge_rank) below kSortMin
+// candidates, otherwise by a sorting network (merge_batch).  The rank merge's
+// binary search and per-candidate loop grow with the list, and on lists of
+// 65-96 slots the sorting network is faster throughout (measured on the
+// 20M-point k=64 sheets).
 #ifndef EGT_KNN_MERGE_MIN
 #define EGT_KNN_MERGE_MIN 3
 #endif
+#ifndef EGT_KNN_SORT_MIN
+#define EGT_KNN_SORT_MIN 24
+#endif
 constexpr int kMergeMin = EGT_KNN_MERGE_MIN;
+constexpr int kSortMin = EGT_KNN_SORT_MIN;
 
 // Offers one batch of candidates (one per lane, `adm` = admitted: d <= thres
 // and d < the list's last slot) to the list.
@@ -69,8 +80,10 @@ constexpr int kMergeMin = EGT_KNN_MERGE_MIN;
 template <bool kExact, int S>
 __device__ __forceinline__ void offer(WarpList<S>& L, float d, int p, bool adm, int lane, float* s_md, int* s_mp) {
     unsigned mask = __ballot_sync(0xffffffffu, adm);
-    if (!kExact && __popc(mask) >= kMergeMin) {
-        merge_batch(L, d, p, adm, lane, s_md, s_mp);
+    const int nb = __popc(mask);
+    if (!kExact && nb >= kMergeMin) {
+        if (S > 2 || nb >= kSortMin) merge_batch(L, d, p, adm, lane, s_md, s_mp);
+        else merge_rank(L, d, p, adm, mask, lane, s_md, s_mp);
         return;
     }
     while (mask) {
@@ -98,6 +111,63 @@ __device__ __forceinline__ bool has_ties(const WarpList<S>& L, int keep, int lan
     return __any_sync(0xffffffffu, bad);
 }
 
+// A flattened candidate sequence over up to 32 point ranges (cells, or row
+// ranges of cells).  After compaction the r-th non-empty range is held by
+// lane r: sequence positions [incl of lane r-1, incl of lane r) map to
+// order[cs + ...].  Lanes >= m hold incl = INT_MAX.
+struct RangeSeq {
+    int incl, cs, m, total;
+};
+
+// Builds the sequence from one range per lane (sz points starting at cs; sz
+// = 0 for none).  s_pref / s_start: 32-int scratch of the calling warp.
+__device__ __forceinline__ RangeSeq range_seq(int sz, int cs, int lane, int* s_pref, int* s_start) {
+    int incl = sz;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const unsigned ne = __ballot_sync(0xffffffffu, sz > 0);
+    RangeSeq q;
+    q.total = __shfl_sync(0xffffffffu, incl, 31);
+    q.m = __popc(ne);
+    __syncwarp();
+    if (sz > 0) {
+        const int r = __popc(ne & ((1u << lane) - 1u));
+        s_pref[r] = incl;
+        s_start[r] = cs;
+    }
+    __syncwarp();
+    q.incl = lane < q.m ? s_pref[lane] : INT_MAX;
+    q.cs = lane < q.m ? s_start[lane] : 0;
+    __syncwarp();  // the scratch may be rewritten by the next sequence
+    return q;
+}
+
+// Point index of candidate base + lane of the sequence (-1 past its end).
+// The range of every lane of the chunk comes from two warp votes: the number
+// of ranges ending at or before `base`, and a mask of the positions inside
+// the chunk where a new range starts.  `order` maps level order to sorted
+// index (nullptr: identity).
+__device__ __forceinline__ int seq_index(const RangeSeq& q, int base, int lane, const int* __restrict__ order) {
+    const int before = __popc(__ballot_sync(0xffffffffu, q.incl <= base));
+    const int at = q.incl - base;
+    const unsigned starts = __reduce_or_sync(0xffffffffu, (at > 0 && at < 32) ? (1u << at) : 0u);
+    const int c = before + __popc(starts & ((2u << lane) - 1u));
+    const int prev_end = __shfl_sync(0xffffffffu, q.incl, (c - 1) & 31);
+    const int cs = __shfl_sync(0xffffffffu, q.cs, c & 31);
+    const int j = base + lane;
+    if (j >= q.total) return -1;
+    const int pos = cs + (j - (c > 0 ? prev_end : 0));
+    return order ? __ldg(order + pos) : pos;
+}
+
+// Position of candidate point p (a dummy for no candidate or the query itself).
+__device__ __forceinline__ float4 stream_point(int p, int q, const float4* __restrict__ p4) {
+    return (p >= 0 && p != q) ? __ldg(p4 + p) : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 // Streams the points of `m` cells (cell l held by lane l as [cs, ce), ce < 0 =
 // empty) through the list, in cell order.  Sets `invalid` when a visited cell
 // holds >= max_pts points (GridKNNCuda.cu:672, 685): the cells before it are
@@ -113,48 +183,36 @@ __device__ __forceinline__ void stream_cells(WarpList<S>& L, bool& invalid, int 
     const bool big = exists && (ce - cs) >= max_pts;
     const unsigned bigmask = __ballot_sync(0xffffffffu, big);
     const int mlim = bigmask ? (__ffs(bigmask) - 1) : m;
-    int sz = (lane < mlim && exists) ? ce - cs : 0;
-    int incl = sz;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    __syncwarp();
-    s_pref[lane] = incl;
-    s_start[lane] = cs;
-    __syncwarp();
+    const int sz = (lane < mlim && exists) ? ce - cs : 0;
+    const RangeSeq seq = range_seq(sz, cs, lane, s_pref, s_start);
     const int qx = (int)((qc0 & 1023u) >> max(skipL, 0)), qy = (int)(((qc0 >> 10) & 1023u) >> max(skipL, 0)),
               qz = (int)(((qc0 >> 20) & 1023u) >> max(skipL, 0));
-    for (int base = 0; base < total; base += 32) {
-        const int j = base + lane;
+    // Software pipeline over 32-candidate chunks: while chunk c is filtered
+    // and offered, the position of chunk c+1 and the point index of chunk c+2
+    // are in flight, so the dependent index -> position loads of a chunk never
+    // wait in line.
+    int pA = seq_index(seq, 32, lane, order);
+    int pB = seq_index(seq, 0, lane, order);
+    float4 vB = stream_point(pB, q, p4);
+    for (int base = 0; base < seq.total; base += 32) {
+        const int p = pB;
+        const float4 v = vB;
+        pB = pA;
+        vB = stream_point(pB, q, p4);
+        pA = seq_index(seq, base + 64, lane, order);
         float d = 1e30f;
-        int p = -1;
         bool ok = false;
-        if (j < total) {
-            int lo = 0, hi = mlim - 1;  // first cell with incl > j
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (s_pref[mid] > j) hi = mid;
-                else lo = mid + 1;
+        if (p >= 0 && p != q) {
+            bool fresh = true;
+            if (skipL >= 0) {
+                const uint32_t c = __float_as_uint(v.w);
+                const int px = (int)((c & 1023u) >> skipL), py = (int)(((c >> 10) & 1023u) >> skipL),
+                          pz = (int)(((c >> 20) & 1023u) >> skipL);
+                fresh = abs(px - qx) > 1 || abs(py - qy) > 1 || abs(pz - qz) > 1;
             }
-            const int excl = lo > 0 ? s_pref[lo - 1] : 0;
-            const int pos = s_start[lo] + (j - excl);
-            p = order ? order[pos] : pos;
-            if (p != q) {
-                const float4 v = p4[p];
-                bool fresh = true;
-                if (skipL >= 0) {
-                    const uint32_t c = __float_as_uint(v.w);
-                    const int px = (int)((c & 1023u) >> skipL), py = (int)(((c >> 10) & 1023u) >> skipL),
-                              pz = (int)(((c >> 20) & 1023u) >> skipL);
-                    fresh = abs(px - qx) > 1 || abs(py - qy) > 1 || abs(pz - qz) > 1;
-                }
-                if (fresh) {
-                    d = fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z);
-                    ok = d <= thres;
-                }
+            if (fresh) {
+                d = fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z);
+                ok = d <= thres;
             }
         }
         offer<kExact, S>(L, d, p, ok && d < L.kth, lane, s_md, s_mp);
