@@ -123,17 +123,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(init: bool = True):
+    """Rank, world size and local rank from the torchrun environment; with
+    init and more than one rank, joins the process group (NCCL with one GPU per
+    rank, gloo when no GPU is present)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if world > 1 and init:
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        timeout = datetime.timedelta(seconds=600)
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timeout, device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=timeout)
     return world, rank, local
 
 
@@ -144,13 +150,21 @@ def barrier(world):
 
 
 def max_over_ranks(world, v: float) -> float:
+    """The largest of the ranks' values (every rank calls it, in the same order)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_rate(world: int, units_per_rank: float, seconds: float) -> float:
+    """Whole-job rate: every rank processes units_per_rank in the time of the
+    slowest rank (weak scaling, replicas of the workload)."""
+    return world * units_per_rank / seconds
 
 
 def cpu_baseline(xyz, k, budget_s=20.0):
@@ -174,7 +188,7 @@ def cpu_baseline(xyz, k, budget_s=20.0):
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    xyz = load_points()
+    xyz = load_points(args.points)
     vals = []
     info = None
     for i in range(args.warmup + args.steps):
@@ -185,8 +199,8 @@ def run_reference(args, world, rank):
     line = {"metric": "Mqueries/s kNN (k=40) + Taubin iters/s at 4M pts; learned vs plain, exact",
             "value": v, "unit": "Mqueries/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "superquadrics 4M points, 50:1 clustered density, k=40 exact grid kNN",
-                       "n_points": N_POINTS, "k": K},
+            "config": {"workload": f"superquadrics {xyz.shape[0]} points, 50:1 clustered density, k=40 exact grid kNN",
+                       "n_points": int(xyz.shape[0]), "k": K},
             "cpu_baseline": dict(info, value=v),
             "e2e": {"value": v, "unit": "Mqueries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -286,7 +300,7 @@ def run_b200(args, world, rank, local):
     ms = max_over_ranks(world, t0.elapsed_time(t1)) / args.steps
     build_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
     knn_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
-    value = world * n / (ms * 1e-3) / 1e6
+    value = aggregate_rate(world, n, ms * 1e-3) / 1e6
     tm = g.timings()
 
     # roofline of the dominant kernel (the kNN query kernel): algorithmic bytes
@@ -345,7 +359,7 @@ def run_b200(args, world, rank, local):
         if i >= args.warmup:
             e2e_times.append(max_over_ranks(world, e))
     e2e_s = statistics.mean(e2e_times)
-    e2e_value = world * n / e2e_s / 1e6
+    e2e_value = aggregate_rate(world, n, e2e_s) / 1e6
 
     if rank == 0:
         line = {
@@ -396,14 +410,15 @@ def main():
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="workload size override (profiling a smaller case of the same step)")
     args = ap.parse_args()
-    world, rank, local = dist_setup()
+    # the reference arm runs on rank 0 alone and needs no process group
+    world, rank, local = dist_setup(init=args.impl != "reference")
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_b200(args, world, rank, local)
     finally:
-        if world > 1:
+        if world > 1 and args.impl != "reference":
             import torch.distributed as dist
             dist.destroy_process_group()
 
