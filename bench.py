@@ -11,7 +11,8 @@ order).  The Taubin loop (EGT filter, then 300 lambda/mu iterations in one
 CUDA graph) is timed in the same run and reported as taubin_iters_per_s with
 its own HBM roofline, followed by the normals and their orientation.  Rank 0
 also compares the proposal-driven kNN with the plain grid kNN on the 20M-point
-k=64 sheets workload (learned_vs_plain; --no-learned skips it).
+k=64 sheets workload (learned_vs_plain; --no-learned skips it) and runs the
+256-cloud batched workload (batched; --no-batched skips it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -257,6 +258,50 @@ def learned_vs_plain(capi):
     return out
 
 
+def batched(capi, iters: int = 150, alpha: float = 0.65):
+    """The batched workload: 256 clouds (noisy spheres and tori) with point
+    counts log-uniform in 2K-500K and k drawn from {10, 20, 40}, seed 4, run
+    through grid build, kNN, EGT filter and `iters` Taubin iterations with one
+    launch per stage (egt_batch_run).  The first run autotunes the work chunk
+    and the Taubin kernel; the best of 3 further runs is reported, stage by
+    stage (CUDA events).  Four sampled clouds are checked against their own
+    single-cloud pipeline, bit for bit."""
+    from multigpuegtsmoothing_b200 import datagen
+    clouds = datagen.batch_clouds(count=256, nmin=2000, nmax=500_000, seed=4)
+    b = capi.Batch(clouds)
+    b.run(iters, alpha=alpha)
+    best = None
+    for _ in range(3):
+        b.run(iters, alpha=alpha)
+        t = b.timings()
+        total = t["grid_ms"] + t["knn_ms"] + t["egt_ms"] + t["taubin_ms"]
+        if best is None or total < best[0]:
+            best = (total, t)
+    total, t = best
+    out = b.output()
+    sample = np.random.default_rng(4).choice(len(clouds), 4, replace=False)
+    same = 0
+    for c in sample:
+        xyz, k = clouds[c]
+        g = capi.GridStructure(xyz)
+        g.GRIDCUDAKNNSELF_COMPACT(k)
+        e = capi.EGT_CUDA(g)
+        e.Filter(alpha)
+        e.Taubin(iters)
+        x, y, z = capi.getOutputPoints(g)
+        g.close()
+        same += bool(np.array_equal(out[c], np.stack([x, y, z], 1)))
+    b.close()
+    n = int(t["points"])
+    return {"workload": f"{len(clouds)} clouds, 2K-500K points log-uniform, k in {{10,20,40}}, "
+                        f"EGT + {iters} Taubin iterations, one launch per stage",
+            "points": n, "grid_ms": t["grid_ms"], "knn_ms": t["knn_ms"], "egt_ms": t["egt_ms"],
+            "taubin_ms": t["taubin_ms"], "total_ms": total, "knn_mqueries_s": n / t["knn_ms"] / 1e3,
+            "taubin_point_iters_per_s": n * iters / (t["taubin_ms"] * 1e-3),
+            "clouds_bit_identical_to_single": f"{same}/{len(sample)}",
+            "knn_chunk": t["knn_chunk"], "taubin_mode": t["taubin_mode"]}
+
+
 def run_b200(args, world, rank, local):
     import torch
     from multigpuegtsmoothing_b200 import capi
@@ -393,6 +438,8 @@ def run_b200(args, world, rank, local):
         }
         if not args.no_learned:
             line["learned_vs_plain"] = learned_vs_plain(capi)
+        if not args.no_batched:
+            line["batched"] = batched(capi)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(xyz, K)
         print(json.dumps(line), flush=True)
@@ -407,6 +454,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal comparison")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-clouds workload")
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="workload size override (profiling a smaller case of the same step)")
     args = ap.parse_args()

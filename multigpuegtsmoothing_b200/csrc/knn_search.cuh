@@ -168,6 +168,32 @@ __device__ __forceinline__ float4 stream_point(int p, int q, const float4* __res
     return (p >= 0 && p != q) ? __ldg(p4 + p) : make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
+// True when no point of the level-L cells x0..x1 of row (cy, cz) can be
+// admitted to the list: the query's distance to their box, less a margin,
+// squared, exceeds the admission threshold kth (admission needs d < kth).
+// Float arithmetic with margins that cover its own rounding: the box bounds
+// are off by ~1e-7 (normalised units), a point may sit ~1e-7 outside its
+// cell's box (the float rounding of its cell key), and the float squared
+// distances carry a relative error below 1e-6; the 2e-6 margin per axis and
+// the 1e-5 relative margin on kth exceed all three, so a skipped row holds no
+// admissible point.  Oversized cells are checked by the caller whatever their
+// distance.
+__device__ __forceinline__ bool cells_beyond(const NormParams& np, float4 pq, int lvl, int x0, int x1, int cy, int cz,
+                                             float kth) {
+    if (!(kth < 1e9f)) return false;  // list not full yet: everything is admitted
+    const float h = __fmul_rn(__fsub_rn(np.b, np.a), (float)(1 << lvl) * (1.0f / 1024.0f));
+    const float c[3] = {pq.x, pq.y, pq.z};
+    const int c0[3] = {x0, cy, cz}, c1[3] = {x1 + 1, cy + 1, cz + 1};
+    float d2 = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const float lo = np.a + (float)c0[d] * h, hi = np.a + (float)c1[d] * h;
+        const float g = fmaxf(fmaxf(lo - c[d], c[d] - hi) - 2e-6f, 0.0f);
+        d2 = fmaf(g, g, d2);
+    }
+    return d2 > kth * (1.0f + 1e-5f);
+}
+
 // Streams the points of `m` cells (cell l held by lane l as [cs, ce), ce < 0 =
 // empty) through the list, in cell order.  Sets `invalid` when a visited cell
 // holds >= max_pts points (GridKNNCuda.cu:672, 685): the cells before it are
@@ -178,12 +204,12 @@ __device__ __forceinline__ void stream_cells(WarpList<S>& L, bool& invalid, int 
                                              const int* __restrict__ order, const float4* __restrict__ p4,
                                              int q, float4 pq, float thres, int max_pts, int lane,
                                              int skipL, uint32_t qc0, int* s_pref, int* s_start, float* s_md,
-                                             int* s_mp) {
+                                             int* s_mp, bool culled = false) {
     const bool exists = lane < m && ce >= 0;
     const bool big = exists && (ce - cs) >= max_pts;
     const unsigned bigmask = __ballot_sync(0xffffffffu, big);
     const int mlim = bigmask ? (__ffs(bigmask) - 1) : m;
-    const int sz = (lane < mlim && exists) ? ce - cs : 0;
+    const int sz = (lane < mlim && exists && !culled) ? ce - cs : 0;
     const RangeSeq seq = range_seq(sz, cs, lane, s_pref, s_start);
     const int qx = (int)((qc0 & 1023u) >> max(skipL, 0)), qy = (int)(((qc0 >> 10) & 1023u) >> max(skipL, 0)),
               qz = (int)(((qc0 >> 20) & 1023u) >> max(skipL, 0));
@@ -244,11 +270,15 @@ __device__ int search(const KnnArgs& a, const NormParams& np, int q, float4 pq, 
         reached = lvl;
         const LevelDev& LV = a.lv[lvl];
         int2 cell = make_int2(-1, -1);
-        if (lane < 26)
-            cell = find_cell(LV, (cx0 >> lvl) + kShell[lane][0], (cy0 >> lvl) + kShell[lane][1],
-                             (cz0 >> lvl) + kShell[lane][2]);
+        bool culled = false;
+        if (lane < 26) {
+            const int cx = (cx0 >> lvl) + kShell[lane][0], cy = (cy0 >> lvl) + kShell[lane][1],
+                      cz = (cz0 >> lvl) + kShell[lane][2];
+            cell = find_cell(LV, cx, cy, cz);
+            culled = cell.x >= 0 && cells_beyond(np, pq, lvl, cx, cx, cy, cz, L.kth);
+        }
         stream_cells<kExact, S>(L, invalid, 26, cell.x, cell.y, LV.order, a.p4, q, pq, np.thres, a.max_pts, lane,
-                                lvl - 1, c0, s_pref, s_start, s_md, s_mp);
+                                lvl - 1, c0, s_pref, s_start, s_md, s_mp, culled);
         cont = decide(np, lvl, 1, L.counter, k, kExact ? L.kth : L.fetch_dist(k - 1), invalid, pq, cx0, cy0, cz0);
         if (lvl == kMaxLevels - 1) break;
     }
