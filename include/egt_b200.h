@@ -138,6 +138,14 @@ egt_status egt_output_device(egt_handle* h, float* x, float* y, float* z, void* 
 /* KNNInterface::GetKNNIndexes (GridKNNCuda.cu:1941-1968): n*k host ints in
  * original ids and original row order. */
 egt_status egt_get_knn_host(egt_handle* h, int* knn_host, void* stream);
+/* egt_knn followed by egt_get_knn_host -- GRIDCUDAKNNSELF_COMPACT(k) then
+ * GetKNNIndexes (GridKNNCuda.cu:2322-2634, :1941-1968) -- with the host copy
+ * overlapped: the queries are searched in chunks of original rows, and each
+ * chunk's rows are copied to knn_host (n*k ints; pinned memory lets the copy
+ * overlap) while the next chunk is searched.  The handle's lists are those
+ * of egt_knn.  In EGT_KNN_LEARNED mode the search and the copy run one after
+ * the other. */
+egt_status egt_knn_host(egt_handle* h, int k, int* knn_host, void* stream);
 /* Device pointers behind the KNNInterface getters. */
 egt_status egt_get_views(egt_handle* h, egt_views* views);
 /* Per-stage device timings of the last calls (filled when the stream is synced). */

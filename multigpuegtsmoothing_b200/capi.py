@@ -92,6 +92,7 @@ def lib() -> C.CDLL:
             "egt_create_cloud_device": (i32, [vp, i64, C.POINTER(Config), vp, hp]),
             "egt_create_mesh": (i32, [vp, i64, vp, i64, C.POINTER(Config), vp, hp]),
             "egt_knn": (i32, [vp, i32, vp]),
+            "egt_knn_host": (i32, [vp, i32, vp, vp]),
             "egt_mesh_1ring": (i32, [vp, i32, vp]),
             "egt_smooth": (i32, [vp, i32, f32, f32, f32, vp]),
             "egt_filter": (i32, [vp, f32, vp]),
@@ -297,6 +298,18 @@ class GridStructure(_Handle):
         if np.float32(thres) != np.float32(1e8):
             raise EgtError(-2, "thres is fixed at creation (config.threshold)")
         _check(lib().egt_knn(self.handle, int(k), self.stream))
+
+    def knn_host(self, k: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """GRIDCUDAKNNSELF_COMPACT(k) then GetKNNIndexes() in one call, with the
+        host copy overlapped with the search (egt_knn_host).  out: optional
+        (n, k) int32 C-contiguous host array (pinned memory overlaps best)."""
+        n = self.pointsRefCount()
+        if out is None:
+            out = np.empty((n, int(k)), np.int32)
+        if out.dtype != np.int32 or out.shape != (n, int(k)) or not out.flags["C_CONTIGUOUS"]:
+            raise EgtError(-2, "knn_host: out must be a C-contiguous (n, k) int32 array")
+        _check(lib().egt_knn_host(self.handle, int(k), _ptr(out), self.stream))
+        return out
 
     def GRIDCUDAKNNSELF_LEARNED(self, k: int, proposal: "SearchProposal"):
         """The same search driven by a learned proposal: lists bit-identical to

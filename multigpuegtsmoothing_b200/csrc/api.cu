@@ -237,6 +237,21 @@ egt_status egt_knn(egt_handle* h, int k, void* stream) {
     return run_knn(h, k);
 }
 
+egt_status egt_knn_host(egt_handle* h, int k, int* knn_host, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (!knn_host) { set_error("egt_knn_host: null output"); return EGT_ERR_ARG; }
+    if (h->is_mesh) { set_error("egt_knn_host: mesh handles take their neighbours from triangles"); return EGT_ERR_STATE; }
+    if ((int64_t)k * h->n > (int64_t)0x7fffffff) { set_error("egt_knn_host: n*k exceeds 2^31-1"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    if (h->cfg.knn_mode == EGT_KNN_LEARNED) {  // no chunked form: search, then copy
+        EGT_TRY(egt_knn(h, k, stream));
+        return egt_get_knn_host(h, knn_host, stream);
+    }
+    h->last_knn_learned = false;
+    return run_knn_host(h, k, knn_host);
+}
+
 egt_status egt_knn_learned(egt_handle* h, int k, const egt_proposal* p, void* stream) {
     EGT_TRY(check_handle(h));
     if (!p) { set_error("egt_knn_learned: null proposal"); return EGT_ERR_ARG; }

@@ -25,7 +25,9 @@
 // time, which never grows (the admission rule rejects it), so offering it again
 // cannot change the list.
 #include <atomic>
+#include <cub/cub.cuh>
 #include <map>
+#include <vector>
 #include <mutex>
 
 #include "egt_internal.cuh"
@@ -52,7 +54,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_plain(KnnArgs a
     const NormParams np = *a.np;
     for (int q0 = claim(a, lane); q0 < a.n; q0 = claim(a, lane)) {
         const int q1 = min(q0 + a.chunk, a.n);
-        for (int q = q0; q < q1; q++) {
+        for (int jq = q0; jq < q1; jq++) {
+            const int q = a.qmap ? a.qmap[jq] : jq;
             const float4 pq = a.p4[q];
             WarpList<S> L;
             bool invalid, rerun;
@@ -447,7 +450,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_learned(KnnArgs
     const NormParams np = *a.np;
     for (int q0 = claim(a, lane); q0 < a.n; q0 = claim(a, lane)) {
         const int q1 = min(q0 + a.chunk, a.n);
-        for (int q = q0; q < q1; q++) {
+        for (int jq = q0; jq < q1; jq++) {
+            const int q = a.qmap ? a.qmap[jq] : jq;
             const float4 pq = a.p4[q];
             WarpList<S> L;
             bool invalid = false, ok = false;
@@ -559,10 +563,10 @@ egt_status level_maxpop(egt_handle* h) {
     return EGT_OK;
 }
 
-egt_status run_knn(egt_handle* h, int k) {
+// Lists and per-query buffers for k, and the search arguments of handle h.
+static egt_status knn_prepare(egt_handle* h, int k, KnnArgs* a) {
     if (k <= 0 || k > 256) { set_error("egt_knn: k must be in [1, 256]"); return EGT_ERR_ARG; }
     if (h->levels_built < kMaxLevels) { set_error("egt_knn: grid hierarchy not built"); return EGT_ERR_STATE; }
-    cudaStream_t st = h->stream;
     const int64_t n = h->n;
     if (h->k != k || !h->lists) {
         if (h->lists) dev_free(h, h->lists);
@@ -573,21 +577,24 @@ egt_status run_knn(egt_handle* h, int k) {
     if (!h->kth) EGT_CUDA_TRY(dev_alloc(h, &h->kth, sizeof(float) * n));
     if (!h->qlevel) EGT_CUDA_TRY(dev_alloc(h, &h->qlevel, n));
     h->have_csr = false;
-    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
-    KnnArgs a;
-    a.p4 = h->p4;
-    a.np = h->d_norm;
-    for (int L = 0; L < kMaxLevels; L++) a.lv[L] = h->lv[L];
-    a.n = (int)n;
-    a.k = k;
-    a.max_pts = h->cfg.max_points_in_cell;
-    a.chunk = kChunk;
-    a.lists = h->lists;
-    a.kth_out = h->kth;
-    a.qlevel = h->qlevel;
-    a.counters = h->d_counters;
-    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, 2 * sizeof(unsigned long long), st));
-    EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
+    a->p4 = h->p4;
+    a->np = h->d_norm;
+    for (int L = 0; L < kMaxLevels; L++) a->lv[L] = h->lv[L];
+    a->n = (int)n;
+    a->k = k;
+    a->max_pts = h->cfg.max_points_in_cell;
+    a->chunk = kChunk;
+    a->lists = h->lists;
+    a->kth_out = h->kth;
+    a->qlevel = h->qlevel;
+    a->counters = h->d_counters;
+    a->qmap = nullptr;
+    return EGT_OK;
+}
+
+// One plain search launch over a.n queries (the work counter must be zero).
+static egt_status knn_launch(const KnnArgs& a, cudaStream_t st) {
+    const int k = a.k;
     // the list keeps k+1 slots (k for k = 256, which always uses the exact rule)
     if (k + 1 <= 32) EGT_TRY((launch<1, true>(a, st)));
     else if (k + 1 <= 64) EGT_TRY((launch<2, true>(a, st)));
@@ -595,8 +602,135 @@ egt_status run_knn(egt_handle* h, int k) {
     else if (k + 1 <= 128) EGT_TRY((launch<4, true>(a, st)));
     else if (k + 1 <= 256) EGT_TRY((launch<8, true>(a, st)));
     else EGT_TRY((launch<8, false>(a, st)));
+    return EGT_OK;
+}
+
+egt_status run_knn(egt_handle* h, int k) {
+    cudaStream_t st = h->stream;
+    KnnArgs a;
+    EGT_TRY(knn_prepare(h, k, &a));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, 2 * sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
+    EGT_TRY(knn_launch(a, st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[3], st));
     return EGT_OK;
+}
+
+namespace {
+// Sort key of sorted slot s for the chunked search: the chunk of its original row.
+__global__ void k_chunk_keys(const int* __restrict__ perm, int n, int rows, uint32_t* __restrict__ key,
+                             int* __restrict__ idx) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    key[s] = (uint32_t)(perm[s] / rows);
+    idx[s] = s;
+}
+
+// Rows of queries qmap[0..m) in original order and ids (GetKNNIndexes layout).
+__global__ void k_rows_original(const int* __restrict__ lists, const int* __restrict__ perm,
+                                const int* __restrict__ qmap, int m, int k, int* __restrict__ out) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= (int64_t)m * k) return;
+    const int j = (int)(e / k), t = (int)(e % k);
+    const int q = qmap[j];
+    const int v = lists[(size_t)q * k + t];
+    out[(size_t)perm[q] * k + t] = v >= 0 ? perm[v] : -1;
+}
+}  // namespace
+
+// The plain search with its lists delivered to the host in original order
+// (egt_knn followed by egt_get_knn_host).  The queries are searched in chunks
+// of original rows: the sorted slots are grouped by the chunk of their
+// original row (a stable sort, so each chunk keeps sorted order and most of
+// its spatial locality).  Chunks alternate between two streams, so one
+// chunk's tail overlaps the next chunk's start, and each finished chunk's
+// rows -- a contiguous block of the original-order output -- are copied to
+// the host on a third stream while later chunks are searched.  The handle's
+// sorted-space lists are filled as egt_knn fills them.
+#ifndef EGT_KNN_HOST_CHUNKS
+#define EGT_KNN_HOST_CHUNKS 8
+#endif
+egt_status run_knn_host(egt_handle* h, int k, int* host) {
+    cudaStream_t st = h->stream;
+    KnnArgs a;
+    EGT_TRY(knn_prepare(h, k, &a));
+    const int n = (int)h->n;
+    const int chunks = std::max(1, std::min(EGT_KNN_HOST_CHUNKS, n / 131072));
+    const int rows = (n + chunks - 1) / chunks;
+    int bits = 1;
+    while ((1 << bits) < chunks) bits++;
+    uint32_t *key = nullptr, *key2 = nullptr;
+    int *idx = nullptr, *qmap = nullptr, *out = nullptr;
+    unsigned long long* work = nullptr;
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&key, sizeof(uint32_t) * n, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&key2, sizeof(uint32_t) * n, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&idx, sizeof(int) * n, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&qmap, sizeof(int) * n, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&out, sizeof(int) * (size_t)n * k, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&work, sizeof(unsigned long long) * chunks, st));
+    EGT_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long) * chunks, st));
+    const unsigned T = 256;
+    k_chunk_keys<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(h->perm, n, rows, key, idx);
+    EGT_LAUNCH_CHECK();
+    size_t t_sort = 0;
+    EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, t_sort, key, key2, idx, qmap, n, 0, bits, st));
+    void* tmp = nullptr;
+    EGT_TRY(scratch_reserve(h, t_sort, &tmp));
+    EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, t_sort, key, key2, idx, qmap, n, 0, bits, st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
+    // streams: [0] = h->stream, [1] = a second search stream, [2] = copies
+    cudaStream_t ss[3] = {st, nullptr, nullptr};
+    std::vector<cudaEvent_t> ev(2 * chunks + 2, nullptr);
+    egt_status s = EGT_OK;
+    auto fail = [&](cudaError_t e, const char* what) {
+        if (e != cudaSuccess && s == EGT_OK) { set_error(cuda_msg(e, what, __FILE__, __LINE__)); s = EGT_ERR_CUDA; }
+    };
+    fail(cudaStreamCreateWithFlags(&ss[1], cudaStreamNonBlocking), "cudaStreamCreate");
+    fail(cudaStreamCreateWithFlags(&ss[2], cudaStreamNonBlocking), "cudaStreamCreate");
+    for (size_t i = 0; i < ev.size() && s == EGT_OK; i++)
+        fail(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming), "cudaEventCreate");
+    // the second search stream starts after the set-up on the first
+    if (s == EGT_OK) fail(cudaEventRecord(ev[2 * chunks], st), "cudaEventRecord");
+    if (s == EGT_OK) fail(cudaStreamWaitEvent(ss[1], ev[2 * chunks], 0), "cudaStreamWaitEvent");
+    for (int c = 0; c < chunks && s == EGT_OK; c++) {
+        const int r0 = c * rows, m = std::min(rows, n - r0);
+        if (m <= 0) break;
+        cudaStream_t cs = ss[c & 1];
+        // the chunk's sorted slots sit at qmap[r0, r0 + m): every chunk holds exactly its row count
+        KnnArgs ac = a;
+        ac.qmap = qmap + r0;
+        ac.n = m;
+        ac.work = work + c;
+        s = knn_launch(ac, cs);
+        if (s != EGT_OK) break;
+        const int64_t cnt = (int64_t)m * k;
+        k_rows_original<<<(unsigned)((cnt + T - 1) / T), T, 0, cs>>>(h->lists, h->perm, qmap + r0, m, k, out);
+        count_launch();
+        fail(cudaGetLastError(), "k_rows_original");
+        if (s == EGT_OK) fail(cudaEventRecord(ev[c], cs), "cudaEventRecord");
+        if (s == EGT_OK) fail(cudaStreamWaitEvent(ss[2], ev[c], 0), "cudaStreamWaitEvent");
+        if (s == EGT_OK)
+            fail(cudaMemcpyAsync(host + (size_t)r0 * k, out + (size_t)r0 * k, sizeof(int) * cnt,
+                                 cudaMemcpyDeviceToHost, ss[2]),
+                 "chunk copy");
+    }
+    // join: the first stream waits for the second search stream, then ends the timing
+    if (s == EGT_OK) fail(cudaEventRecord(ev[2 * chunks + 1], ss[1]), "cudaEventRecord");
+    if (s == EGT_OK) fail(cudaStreamWaitEvent(st, ev[2 * chunks + 1], 0), "cudaStreamWaitEvent");
+    if (s == EGT_OK) fail(cudaEventRecord(h->ev[3], st), "cudaEventRecord");
+    fail(cudaStreamSynchronize(ss[2]), "copy stream");
+    fail(cudaStreamSynchronize(ss[1]), "search stream");
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    if (ss[1]) cudaStreamDestroy(ss[1]);
+    if (ss[2]) cudaStreamDestroy(ss[2]);
+    cudaFreeAsync(key, st); cudaFreeAsync(key2, st); cudaFreeAsync(idx, st); cudaFreeAsync(qmap, st);
+    cudaFreeAsync(out, st); cudaFreeAsync(work, st);
+    fail(cudaStreamSynchronize(st), "stream");
+    return s;
 }
 
 egt_status run_knn_learned(egt_handle* h, int k, const egt_proposal* p) {

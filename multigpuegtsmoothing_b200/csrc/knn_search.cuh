@@ -19,6 +19,8 @@ struct KnnArgs {
     float* __restrict__ kth_out;
     uint8_t* __restrict__ qlevel;
     unsigned long long* __restrict__ counters;
+    const int* __restrict__ qmap = nullptr;  // query j of a launch is qmap[j] (nullptr: j)
+    unsigned long long* __restrict__ work = nullptr;  // work counter (nullptr: counters[kCtrWork])
 };
 
 constexpr int kWarps = 8;
@@ -328,7 +330,7 @@ constexpr int kChunk = 4;
 // Next chunk of queries for the calling warp (uniform); >= n when done.
 __device__ __forceinline__ int claim(const KnnArgs& a, int lane) {
     unsigned long long q0 = 0;
-    if (lane == 0) q0 = atomicAdd(&a.counters[kCtrWork], (unsigned long long)a.chunk);
+    if (lane == 0) q0 = atomicAdd(a.work ? a.work : &a.counters[kCtrWork], (unsigned long long)a.chunk);
     return (int)min(__shfl_sync(0xffffffffu, q0, 0), (unsigned long long)a.n);
 }
 

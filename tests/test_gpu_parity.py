@@ -175,3 +175,23 @@ def test_superquadrics_4m_digest(capi):
     assert sha(g.sorted_lists()) == dg["ref_knn_raw"]
     capi.EGT_CUDA(g).Filter(m["alpha"])
     assert sha(g.sorted_lists()) == dg["ref_knn_egt"]
+
+
+def test_chunked_knn_host_matches_search_then_copy(capi):
+    """egt_knn_host (search in chunks of original rows, host copies overlapped)
+    returns what egt_knn + egt_get_knn_host return, and leaves the same
+    sorted-space lists on the handle; 600K points run as 4 chunks."""
+    xyz = datagen.superquadrics(600_000, seed=7)
+    g = cloud(capi, xyz, 40)
+    want = g.GetKNNIndexes()
+    lists = g.sorted_lists()
+    t = g.timings()
+    g2 = capi.GridStructure(xyz)
+    got = g2.knn_host(40)
+    assert np.array_equal(got, want)
+    assert np.array_equal(g2.sorted_lists(), lists)
+    t2 = g2.timings()
+    assert t2["invalid_queries"] == t["invalid_queries"] and t2["levels_used"] == t["levels_used"]
+    # a second call on the same handle (buffers reused)
+    assert np.array_equal(g2.knn_host(40), want)
+    g2.close()
