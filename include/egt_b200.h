@@ -146,6 +146,16 @@ egt_status egt_get_knn_host(egt_handle* h, int* knn_host, void* stream);
  * of egt_knn.  In EGT_KNN_LEARNED mode the search and the copy run one after
  * the other. */
 egt_status egt_knn_host(egt_handle* h, int k, int* knn_host, void* stream);
+
+/* Query-vs-reference kNN against the handle's points:
+ * GridStructure::GRIDCUDAKNNCompact(qx, qy, qz, nq, k, thres) then
+ * GetKNNIndexes (GridKNNCuda.cu:1645-1968).  queries_host: nq*3 floats (AoS,
+ * the reference's units; they may lie outside its cube); knn_host: nq*k ints,
+ * original reference ids in query order, -1 padded (an invalid query's row is
+ * all -1); invalid (optional): number of invalid queries.  thres is the
+ * handle's configured threshold.  The handle's own lists are not changed. */
+egt_status egt_knn_query(egt_handle* h, const float* queries_host, int64_t nq, int k, int* knn_host,
+                         int64_t* invalid, void* stream);
 /* Device pointers behind the KNNInterface getters. */
 egt_status egt_get_views(egt_handle* h, egt_views* views);
 /* Per-stage device timings of the last calls (filled when the stream is synced). */

@@ -11,6 +11,7 @@
 #define EGT_KNN_INTERFACE_HPP
 
 #include <cstdint>
+#include <algorithm>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -121,8 +122,37 @@ public:
     void GRIDCUDAKNNSELF_COMPACT(int k, float thres = 1e8f) {
         if (thres != 1e8f) throw Error(EGT_ERR_ARG, "GRIDCUDAKNNSELF_COMPACT: thres is fixed at 1e8");
         check(egt_knn(h_, k, stream_), "GRIDCUDAKNNSELF_COMPACT");
+        query_.clear();
+        nq_ = -1;
         refresh();
     }
+    // GridStructure::GRIDCUDAKNNCompact (GridKNNCuda.cu:1645-1939): the k
+    // nearest reference points of nq query points (host SoA, the reference's
+    // units).  As in the reference, GetKNNIndexes then returns the query
+    // lists (nq rows in query order) until the next self search.
+    void GRIDCUDAKNNCompact(const float* qx, const float* qy, const float* qz, int nq, int k, float thres = 1e8f) {
+        if (thres != 1e8f) throw Error(EGT_ERR_ARG, "GRIDCUDAKNNCompact: thres is fixed at 1e8");
+        std::vector<float> q(3 * (size_t)nq);
+        for (int i = 0; i < nq; i++) {
+            q[3 * (size_t)i] = qx[i];
+            q[3 * (size_t)i + 1] = qy[i];
+            q[3 * (size_t)i + 2] = qz[i];
+        }
+        query_.assign((size_t)nq * k, -1);
+        check(egt_knn_query(h_, q.data(), nq, k, query_.data(), nullptr, stream_), "GRIDCUDAKNNCompact");
+        nq_ = nq;
+        qk_ = k;
+    }
+    void GetKNNIndexes(int* knn) override {
+        if (nq_ < 0) return Provider::GetKNNIndexes(knn);
+        std::copy(query_.begin(), query_.end(), knn);
+    }
+    [[nodiscard]] int pointsQuerCount() const override { return nq_ < 0 ? pointsRefCount() : nq_; }
+    [[nodiscard]] int NeighborCount() const override { return nq_ < 0 ? Provider::NeighborCount() : qk_; }
+
+private:
+    std::vector<int> query_;
+    int nq_ = -1, qk_ = 0;
 };
 
 // GridMeshCuda(mesh, num_cards, eps, bucketCount) + GetNeighborsFromTriangles.

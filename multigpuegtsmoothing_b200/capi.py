@@ -93,6 +93,7 @@ def lib() -> C.CDLL:
             "egt_create_mesh": (i32, [vp, i64, vp, i64, C.POINTER(Config), vp, hp]),
             "egt_knn": (i32, [vp, i32, vp]),
             "egt_knn_host": (i32, [vp, i32, vp, vp]),
+            "egt_knn_query": (i32, [vp, vp, i64, i32, vp, C.POINTER(C.c_int64), vp]),
             "egt_mesh_1ring": (i32, [vp, i32, vp]),
             "egt_smooth": (i32, [vp, i32, f32, f32, f32, vp]),
             "egt_filter": (i32, [vp, f32, vp]),
@@ -310,6 +311,16 @@ class GridStructure(_Handle):
             raise EgtError(-2, "knn_host: out must be a C-contiguous (n, k) int32 array")
         _check(lib().egt_knn_host(self.handle, int(k), _ptr(out), self.stream))
         return out
+
+    def GRIDCUDAKNNCompact(self, queries: np.ndarray, k: int) -> Tuple[np.ndarray, int]:
+        """Query-vs-reference kNN (GridKNNCuda.cu:1645-1968) against this
+        provider's points: (nq, k) int32 original reference ids in query order
+        (GetKNNIndexes layout) and the number of invalid queries."""
+        q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, 3)
+        out = np.empty((q.shape[0], int(k)), np.int32)
+        inv = C.c_int64(0)
+        _check(lib().egt_knn_query(self.handle, _ptr(q), q.shape[0], int(k), _ptr(out), C.byref(inv), self.stream))
+        return out, int(inv.value)
 
     def GRIDCUDAKNNSELF_LEARNED(self, k: int, proposal: "SearchProposal"):
         """The same search driven by a learned proposal: lists bit-identical to

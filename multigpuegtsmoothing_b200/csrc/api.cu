@@ -252,6 +252,15 @@ egt_status egt_knn_host(egt_handle* h, int k, int* knn_host, void* stream) {
     return run_knn_host(h, k, knn_host);
 }
 
+egt_status egt_knn_query(egt_handle* h, const float* queries_host, int64_t nq, int k, int* knn_host,
+                         int64_t* invalid, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (h->is_mesh) { set_error("egt_knn_query: point-cloud handles only"); return EGT_ERR_STATE; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    return run_knn_query(h, queries_host, nq, k, knn_host, invalid);
+}
+
 egt_status egt_knn_learned(egt_handle* h, int k, const egt_proposal* p, void* stream) {
     EGT_TRY(check_handle(h));
     if (!p) { set_error("egt_knn_learned: null proposal"); return EGT_ERR_ARG; }

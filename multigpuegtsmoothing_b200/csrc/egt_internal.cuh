@@ -213,6 +213,7 @@ egt_status scratch_reserve(egt_handle* h, size_t bytes, void** out);
 egt_status build_grid(egt_handle* h, const float* xyz_dev_aos, int levels);
 egt_status run_knn(egt_handle* h, int k);
 egt_status run_knn_host(egt_handle* h, int k, int* host);
+egt_status run_knn_query(egt_handle* h, const float* q_host, int64_t nq, int k, int* out_host, int64_t* invalid);
 egt_status run_knn_learned(egt_handle* h, int k, const egt_proposal* p);
 int proposal_k(const egt_proposal* p);
 int proposal_device(const egt_proposal* p);

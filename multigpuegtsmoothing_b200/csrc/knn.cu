@@ -482,6 +482,139 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_learned(KnnArgs
     if (threadIdx.x == 0 && s_rerun) atomicAdd(&a.counters[kCtrExactRerun], (unsigned long long)s_rerun);
 }
 
+// ---------------------------------------------------------------------------
+// Query-vs-reference kNN: GridStructure::GRIDCUDAKNNCompact (GridKNNCuda.cu:
+// 1645-1939) with its kernel construct_neighbors (GridKNNCuda.cu:340-438) and
+// GetKNNIndexes (:1941-1968).  The schedule is the self search's (own level-0
+// cell, then the 26-cell shell at levels 0..7, invalid when still searching
+// after B = 8), with the reference's differences for foreign queries:
+//   * a query is normalised with the reference cloud's cube and may lie
+//     outside it; its cell at level L is (int)(u * B_L), u = (x - a)/(b - a)
+//     (:349-351), truncated toward zero, so it is computed per level rather
+//     than shifted from level 0;
+//   * no point is excluded as "self", and admission is d < thres (:357-363);
+//   * with fewer than k neighbours the search continues when sqrt(thres) >=
+//     a face distance (:377-392; the self search uses >);
+//   * cells outside the grid are skipped without invalidating (:352-354).
+__device__ __forceinline__ bool decide_query(const NormParams& np, int L, int o, int counter, int k, float kth,
+                                             bool invalid, float4 q, const int ci[3]) {
+    if (invalid) return false;
+    const int B = 1024 >> L;
+    const float h = __fdiv_rn(__fsub_rn(np.b, np.a), (float)B);
+    const float c[3] = {q.x, q.y, q.z};
+    const float r = counter < k ? __fsqrt_rn(np.thres) : __fsqrt_rn(kth);
+    bool more = false;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        more |= (ci[d] - o >= 0) && r >= fs_face_lo(c[d], np.a, (float)(ci[d] - o), h);
+        more |= (ci[d] + o + 1 <= B) && r >= fs_face_hi(c[d], np.a, (float)(ci[d] + o + 1), h);
+    }
+    return more;
+}
+
+template <bool kExact, int S>
+__device__ int search_query(const KnnArgs& a, const NormParams& np, float4 pq, const float u[3], float thres_lt,
+                            WarpList<S>& L, bool& invalid, int lane, int* s_pref, int* s_start, float* s_md,
+                            int* s_mp) {
+    const int k = a.k;
+    L.init(kExact ? k : k + 1);
+    invalid = false;
+    int ci[3], cp[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) ci[d] = (int)__fmul_rn(u[d], 1024.0f);
+    int2 own = lane == 0 ? find_cell(a.lv[0], ci[0], ci[1], ci[2]) : make_int2(-1, -1);
+    stream_cells<kExact, S>(L, invalid, 1, own.x, own.y, nullptr, a.p4, -1, pq, thres_lt, a.max_pts, lane, -1, 0, 0,
+                            0, s_pref, s_start, s_md, s_mp);
+    bool cont = decide_query(np, 0, 0, L.counter, k, kExact ? L.kth : L.fetch_dist(k - 1), invalid, pq, ci);
+    int reached = 0;
+    for (int lvl = 0; cont; lvl++) {
+        reached = lvl;
+        const LevelDev& LV = a.lv[lvl];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            cp[d] = (int)__fmul_rn(u[d], (float)(1024 >> max(lvl - 1, 0)));  // the block visited so far
+            ci[d] = (int)__fmul_rn(u[d], (float)(1024 >> lvl));
+        }
+        int2 cell = make_int2(-1, -1);
+        bool culled = false;
+        if (lane < 26) {
+            const int cx = ci[0] + kShell[lane][0], cy = ci[1] + kShell[lane][1], cz = ci[2] + kShell[lane][2];
+            cell = find_cell(LV, cx, cy, cz);
+            culled = cell.x >= 0 && cells_beyond(np, pq, lvl, cx, cx, cy, cz, L.kth);
+        }
+        stream_cells<kExact, S>(L, invalid, 26, cell.x, cell.y, LV.order, a.p4, -1, pq, thres_lt, a.max_pts, lane,
+                                lvl - 1, cp[0], cp[1], cp[2], s_pref, s_start, s_md, s_mp, culled);
+        cont = decide_query(np, lvl, 1, L.counter, k, kExact ? L.kth : L.fetch_dist(k - 1), invalid, pq, ci);
+        if (lvl == kMaxLevels - 1) break;
+    }
+    if (cont) { invalid = true; reached = kMaxLevels; }
+    return reached;
+}
+
+// qpos: normalised query positions; query j (processing order a.qmap[j]) is
+// row a.qmap[j] of out, in original reference ids (perm), -1 padded; an
+// invalid query's row is all -1 (negateNotValidKnnIndexes, :291-302).
+template <int S>
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_query(KnnArgs a, const float4* __restrict__ qpos,
+                                                                     const int* __restrict__ perm,
+                                                                     int* __restrict__ out) {
+    __shared__ int s_pref[kWarps][32];
+    __shared__ int s_start[kWarps][32];
+    __shared__ float s_md[kWarps][32 * S];
+    __shared__ int s_mp[kWarps][32 * S];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const NormParams np = *a.np;
+    const float thres_lt = nextafterf(np.thres, 0.0f);  // d <= thres_lt  <=>  d < thres
+    const float ab = __fsub_rn(np.b, np.a);
+    for (int q0 = claim(a, lane); q0 < a.n; q0 = claim(a, lane)) {
+        const int q1 = min(q0 + a.chunk, a.n);
+        for (int jq = q0; jq < q1; jq++) {
+            const int row = a.qmap[jq];
+            const float4 pq = qpos[row];
+            const float u[3] = {__fdiv_rn(__fsub_rn(pq.x, np.a), ab), __fdiv_rn(__fsub_rn(pq.y, np.a), ab),
+                                __fdiv_rn(__fsub_rn(pq.z, np.a), ab)};
+            WarpList<S> L;
+            bool invalid;
+            search_query<false, S>(a, np, pq, u, thres_lt, L, invalid, lane, s_pref[w], s_start[w], s_md[w], s_mp[w]);
+            if (has_ties(L, min(L.counter, a.k + 1), lane)) {
+                search_query<true, S>(a, np, pq, u, thres_lt, L, invalid, lane, s_pref[w], s_start[w], s_md[w],
+                                      s_mp[w]);
+                if (lane == 0) atomicAdd(&a.counters[kCtrExactRerun], 1ull);
+            }
+#pragma unroll
+            for (int s = 0; s < S; s++) {
+                const int t = lane + 32 * s;
+                if (t < a.k) {
+                    const int v = L.idx[s];
+                    out[(size_t)row * a.k + t] = (invalid || v < 0) ? -1 : perm[v];
+                }
+            }
+            if (lane == 0 && invalid) atomicAdd(&a.counters[kCtrInvalid], 1ull);
+        }
+    }
+}
+
+// Normalised query positions (normalize_points, GridKNNCuda.cu:841-849, with
+// the reference cloud's cube) and their level-0 cell keys for the processing
+// order (cells outside the grid clamp to its border: order only).
+__global__ void k_query_prepare(const float* __restrict__ xyz, int nq, const NormParams* __restrict__ np,
+                                float4* __restrict__ qpos, uint32_t* __restrict__ key, int* __restrict__ idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    const float mn = np->mn, d = __fsub_rn(np->mx, np->mn);
+    float4 p;
+    p.x = __fdiv_rn(__fsub_rn(xyz[3 * (size_t)i], mn), d);
+    p.y = __fdiv_rn(__fsub_rn(xyz[3 * (size_t)i + 1], mn), d);
+    p.z = __fdiv_rn(__fsub_rn(xyz[3 * (size_t)i + 2], mn), d);
+    p.w = 0.0f;
+    qpos[i] = p;
+    const int cx = min(max(cell_coord(p.x, np->a, np->b, 1024), 0), 1023);
+    const int cy = min(max(cell_coord(p.y, np->a, np->b, 1024), 0), 1023);
+    const int cz = min(max(cell_coord(p.z, np->a, np->b, 1024), 0), 1023);
+    key[i] = (uint32_t)cx | ((uint32_t)cy << 10) | ((uint32_t)cz << 20);
+    idx[i] = i;
+}
+
 // Blocks of one resident wave of a persistent kernel, per (kernel, device).
 template <typename K>
 egt_status wave_blocks(K kernel, int64_t n, unsigned* out, size_t dyn_smem = 0) {
@@ -730,6 +863,89 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
     cudaFreeAsync(key, st); cudaFreeAsync(key2, st); cudaFreeAsync(idx, st); cudaFreeAsync(qmap, st);
     cudaFreeAsync(out, st); cudaFreeAsync(work, st);
     fail(cudaStreamSynchronize(st), "stream");
+    return s;
+}
+
+template <int S>
+static egt_status launch_query(const KnnArgs& a, const float4* qpos, const int* perm, int* out, cudaStream_t st) {
+    unsigned G = 0;
+    EGT_TRY(wave_blocks(k_knn_query<S>, a.n, &G));
+    k_knn_query<S><<<G, kWarps * 32, 0, st>>>(a, qpos, perm, out);
+    EGT_LAUNCH_CHECK();
+    return EGT_OK;
+}
+
+// Query-vs-reference kNN against handle h's grid (GRIDCUDAKNNCompact +
+// GetKNNIndexes): q_host [nq*3] AoS query points in the reference's units,
+// out_host [nq*k] original reference ids in original query order.  The
+// handle's own lists and statistics are untouched.  Queries are processed in
+// the order of their level-0 cell (the reference also sorts them by cell,
+// GridKNNCuda.cu:1208-1267; the order does not change any result).
+egt_status run_knn_query(egt_handle* h, const float* q_host, int64_t nq, int k, int* out_host, int64_t* invalid) {
+    if (k <= 0 || k > 255) { set_error("egt_knn_query: k must be in [1, 255]"); return EGT_ERR_ARG; }
+    if (nq < 0 || nq > 0x7fffffff || (nq > 0 && (!q_host || !out_host))) {
+        set_error("egt_knn_query: bad query arguments");
+        return EGT_ERR_ARG;
+    }
+    if ((int64_t)k * nq > (int64_t)0x7fffffff) { set_error("egt_knn_query: nq*k exceeds 2^31-1"); return EGT_ERR_ARG; }
+    if (h->levels_built < kMaxLevels) { set_error("egt_knn_query: grid hierarchy not built"); return EGT_ERR_STATE; }
+    if (invalid) *invalid = 0;
+    if (nq == 0) return EGT_OK;
+    cudaStream_t st = h->stream;
+    const int n = (int)nq;
+    float* dq = nullptr;
+    float4* qpos = nullptr;
+    uint32_t *key = nullptr, *key2 = nullptr;
+    int *idx = nullptr, *qmap = nullptr, *out = nullptr;
+    unsigned long long* ctr = nullptr;
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&dq, sizeof(float) * 3 * (size_t)n, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&qpos, sizeof(float4) * n, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&key, sizeof(uint32_t) * n, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&key2, sizeof(uint32_t) * n, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&idx, sizeof(int) * n, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&qmap, sizeof(int) * n, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&out, sizeof(int) * (size_t)n * k, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&ctr, sizeof(unsigned long long) * kCtrWords, st));
+    EGT_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * kCtrWords, st));
+    EGT_CUDA_TRY(cudaMemcpyAsync(dq, q_host, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, st));
+    const unsigned T = 256;
+    k_query_prepare<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(dq, n, h->d_norm, qpos, key, idx);
+    EGT_LAUNCH_CHECK();
+    size_t t_sort = 0;
+    EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, t_sort, key, key2, idx, qmap, n, 0, 30, st));
+    void* tmp = nullptr;
+    EGT_TRY(scratch_reserve(h, t_sort, &tmp));
+    EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, t_sort, key, key2, idx, qmap, n, 0, 30, st));
+    KnnArgs a;
+    a.p4 = h->p4;
+    a.np = h->d_norm;
+    for (int L = 0; L < kMaxLevels; L++) a.lv[L] = h->lv[L];
+    a.n = n;
+    a.k = k;
+    a.max_pts = h->cfg.max_points_in_cell;
+    a.chunk = kChunk;
+    a.lists = nullptr;
+    a.kth_out = nullptr;
+    a.qlevel = nullptr;
+    a.counters = ctr;
+    a.qmap = qmap;
+    egt_status s;
+    if (k + 1 <= 32) s = launch_query<1>(a, qpos, h->perm, out, st);
+    else if (k + 1 <= 64) s = launch_query<2>(a, qpos, h->perm, out, st);
+    else if (k + 1 <= 96) s = launch_query<3>(a, qpos, h->perm, out, st);
+    else if (k + 1 <= 128) s = launch_query<4>(a, qpos, h->perm, out, st);
+    else s = launch_query<8>(a, qpos, h->perm, out, st);
+    unsigned long long inv = 0;
+    if (s == EGT_OK) {
+        cudaError_t e = cudaMemcpyAsync(out_host, out, sizeof(int) * (size_t)n * k, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&inv, ctr + kCtrInvalid, sizeof(inv), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) { set_error(cuda_msg(e, "query results", __FILE__, __LINE__)); s = EGT_ERR_CUDA; }
+    }
+    cudaFreeAsync(dq, st); cudaFreeAsync(qpos, st); cudaFreeAsync(key, st); cudaFreeAsync(key2, st);
+    cudaFreeAsync(idx, st); cudaFreeAsync(qmap, st); cudaFreeAsync(out, st); cudaFreeAsync(ctr, st);
+    const cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess && s == EGT_OK) { set_error(cuda_msg(e, "egt_knn_query", __FILE__, __LINE__)); s = EGT_ERR_CUDA; }
+    if (s == EGT_OK && invalid) *invalid = (int64_t)inv;
     return s;
 }
 

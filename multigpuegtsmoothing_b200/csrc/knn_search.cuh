@@ -200,12 +200,13 @@ __device__ __forceinline__ bool cells_beyond(const NormParams& np, float4 pq, in
 // empty) through the list, in cell order.  Sets `invalid` when a visited cell
 // holds >= max_pts points (GridKNNCuda.cu:672, 685): the cells before it are
 // still processed, the rest are not.  skipL >= 0: skip points whose level-skipL
-// cell lies in the 3x3x3 block around the query's (already visited).
+// cell lies in the 3x3x3 block around the query's level-skipL cell (qx, qy,
+// qz), which the previous levels visited.
 template <bool kExact, int S>
 __device__ __forceinline__ void stream_cells(WarpList<S>& L, bool& invalid, int m, int cs, int ce,
                                              const int* __restrict__ order, const float4* __restrict__ p4,
                                              int q, float4 pq, float thres, int max_pts, int lane,
-                                             int skipL, uint32_t qc0, int* s_pref, int* s_start, float* s_md,
+                                             int skipL, int qx, int qy, int qz, int* s_pref, int* s_start, float* s_md,
                                              int* s_mp, bool culled = false) {
     const bool exists = lane < m && ce >= 0;
     const bool big = exists && (ce - cs) >= max_pts;
@@ -213,8 +214,6 @@ __device__ __forceinline__ void stream_cells(WarpList<S>& L, bool& invalid, int 
     const int mlim = bigmask ? (__ffs(bigmask) - 1) : m;
     const int sz = (lane < mlim && exists && !culled) ? ce - cs : 0;
     const RangeSeq seq = range_seq(sz, cs, lane, s_pref, s_start);
-    const int qx = (int)((qc0 & 1023u) >> max(skipL, 0)), qy = (int)(((qc0 >> 10) & 1023u) >> max(skipL, 0)),
-              qz = (int)(((qc0 >> 20) & 1023u) >> max(skipL, 0));
     // Software pipeline over 32-candidate chunks: while chunk c is filtered
     // and offered, the position of chunk c+1 and the point index of chunk c+2
     // are in flight, so the dependent index -> position loads of a chunk never
@@ -264,7 +263,7 @@ __device__ int search(const KnnArgs& a, const NormParams& np, int q, float4 pq, 
     invalid = false;
     // offset 0 at level 0: the query's own cell (always occupied)
     int2 own = lane == 0 ? find_cell(a.lv[0], cx0, cy0, cz0) : make_int2(-1, -1);
-    stream_cells<kExact, S>(L, invalid, 1, own.x, own.y, nullptr, a.p4, q, pq, np.thres, a.max_pts, lane, -1, c0,
+    stream_cells<kExact, S>(L, invalid, 1, own.x, own.y, nullptr, a.p4, q, pq, np.thres, a.max_pts, lane, -1, 0, 0, 0,
                             s_pref, s_start, s_md, s_mp);
     bool cont = decide(np, 0, 0, L.counter, k, kExact ? L.kth : L.fetch_dist(k - 1), invalid, pq, cx0, cy0, cz0);
     int reached = 0;
@@ -279,8 +278,9 @@ __device__ int search(const KnnArgs& a, const NormParams& np, int q, float4 pq, 
             cell = find_cell(LV, cx, cy, cz);
             culled = cell.x >= 0 && cells_beyond(np, pq, lvl, cx, cx, cy, cz, L.kth);
         }
+        const int sL = max(lvl - 1, 0);
         stream_cells<kExact, S>(L, invalid, 26, cell.x, cell.y, LV.order, a.p4, q, pq, np.thres, a.max_pts, lane,
-                                lvl - 1, c0, s_pref, s_start, s_md, s_mp, culled);
+                                lvl - 1, cx0 >> sL, cy0 >> sL, cz0 >> sL, s_pref, s_start, s_md, s_mp, culled);
         cont = decide(np, lvl, 1, L.counter, k, kExact ? L.kth : L.fetch_dist(k - 1), invalid, pq, cx0, cy0, cz0);
         if (lvl == kMaxLevels - 1) break;
     }

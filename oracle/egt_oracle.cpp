@@ -234,6 +234,96 @@ int knn_query(const Grid& g, int q, int k, float thres, float* dist, int* idx, i
 }
 
 // ---------------------------------------------------------------------------
+// Query-vs-reference kNN: GridStructure::GRIDCUDAKNNCompact (GridKNNCuda.cu:
+// 1645-1939) with its kernel construct_neighbors (GridKNNCuda.cu:340-438).
+// The same level/shell schedule as the self search (own level-0 cell, then the
+// 26-cell shell at levels 0..7, a query still searching after B = 8 is
+// invalid), with these differences, each from the cited lines:
+//   * the query points are normalised with the reference cloud's cube
+//     (normalize_points, :841-849; :1700-1706) and may lie outside it;
+//   * the query's cell at each level is computed from its coordinate,
+//     (int)((x - a)/(b - a) * B_L) (:349-351), which truncates toward zero
+//     for coordinates below the cube;
+//   * no point is excluded as "self" (:357-365);
+//   * admission is dist < thres (:363), strict;
+//   * with fewer than k neighbours the search continues when
+//     sqrt(thres) >= a face distance (:377-392), otherwise when
+//     sqrt(k-th) >= a face distance (:393-420);
+//   * cells outside the grid are skipped, never invalidating (:352-354, :370-374);
+//   * an oversized cell invalidates the query (:367-369).
+// lists: [k] reference sorted-space ids of query (x, y, z), normalised.
+struct QueryCells { int c[kLevels][3]; };
+
+inline QueryCells query_cells(const Grid& g, float x, float y, float z) {
+    QueryCells qc;
+    for (int L = 0; L < kLevels; L++) {
+        const int B = kBuckets >> L;
+        qc.c[L][0] = cell_coord(x, g.a, g.b, B);
+        qc.c[L][1] = cell_coord(y, g.a, g.b, B);
+        qc.c[L][2] = cell_coord(z, g.a, g.b, B);
+    }
+    return qc;
+}
+
+bool decide_more_query(const Grid& g, const QueryCells& qc, float x, float y, float z, int L, int o, int counter,
+                       int k, float kth, float thres) {
+    const int B = g.lv[L].B;
+    const float h = (g.b - g.a) / (float)B;
+    const float c[3] = {x, y, z};
+    const float xmin = g.a;
+    const float r = counter < k ? std::sqrt(thres) : std::sqrt(kth);
+    for (int d = 0; d < 3; d++) {
+        const int ci = qc.c[L][d];
+        if (ci - o >= 0 && r >= face_lo(c[d], xmin, (float)(ci - o), h)) return true;
+        if (ci + o + 1 <= B && r >= face_hi(c[d], xmin, (float)(ci + o + 1), h)) return true;
+    }
+    return false;
+}
+
+int knn_foreign_query(const Grid& g, float xq, float yq, float zq, int k, float thres, float* dist, int* idx,
+                      int& counter, bool& invalid) {
+    for (int i = 0; i < k; i++) { dist[i] = 1e10f; idx[i] = -1; }
+    counter = 0;
+    invalid = false;
+    const QueryCells qc = query_cells(g, xq, yq, zq);
+    auto visit = [&](int L, int cx, int cy, int cz) {
+        const auto& lv = g.lv[L];
+        if (cx < 0 || cx >= lv.B || cy < 0 || cy >= lv.B || cz < 0 || cz >= lv.B) return;
+        const int key = cx + cy * lv.B + cz * lv.B * lv.B;
+        auto it = std::lower_bound(lv.keys.begin(), lv.keys.end(), key);
+        if (it == lv.keys.end() || *it != key) return;
+        if (invalid) return;
+        const size_t c = it - lv.keys.begin();
+        const int s0 = lv.start[c], s1 = lv.start[c + 1];
+        if (s1 - s0 >= kMaxPointsInCube) { invalid = true; return; }
+        for (int j = s0; j < s1; j++) {
+            const int p = lv.order[j];
+            const float d = dist3(xq, yq, zq, g.x[p], g.y[p], g.z[p]);
+            if (d < thres) append(dist, idx, k, counter, d, p);
+        }
+    };
+    auto decide = [&](int L, int o) -> bool {
+        if (invalid) return false;
+        return decide_more_query(g, qc, xq, yq, zq, L, o, counter, k, dist[k - 1], thres);
+    };
+    visit(0, qc.c[0][0], qc.c[0][1], qc.c[0][2]);
+    bool cont = decide(0, 0);
+    int L = 0, reached = 0;
+    while (cont) {
+        reached = L;
+        for (int s = 0; s < 26; s++)
+            visit(L, qc.c[L][0] + kShell[s][0], qc.c[L][1] + kShell[s][1], qc.c[L][2] + kShell[s][2]);
+        cont = decide(L, 1);
+        if (L == kLevels - 1) break;
+        L++;
+    }
+    if (cont) { invalid = true; reached = kLevels; }  // GridKNNCuda.cu:1921-1928
+    if (invalid)
+        for (int i = 0; i < k; i++) idx[i] = -1;
+    return reached;
+}
+
+// ---------------------------------------------------------------------------
 // Learned search proposal (an extension of this project; the reference has no
 // counterpart).  A proposal class names a box of level-L cells of half-width R
 // around the query's level-L cell; the last class means "run the plain search".
@@ -699,6 +789,44 @@ int orc_knn(const float* xyz, int n, int k, int* lists, float* pos, int* perm, f
     }
     ext[0] = g.mn; ext[1] = g.mx;
     if (visited_total) *visited_total = visited_sum;
+    return invalid_count;
+}
+
+// Query-vs-reference kNN of the reference (GridStructure(ref) +
+// GRIDCUDAKNNCompact(queries, k, thres) + GetKNNIndexes, GridKNNCuda.cu:
+// 1645-1968): out [nq*k] original reference ids in original query order, -1
+// padded (whole row -1 for an invalid query).  Returns the invalid count.
+//   status [nq] (optional): 0 = valid, 1 = a visited cell was oversized,
+//   2 = still searching after the B = 8 shell.  The reference decides the
+//   status-2 rows from a buffer it re-allocates without clearing
+//   (recomputeBuffers, GridKNNCuda.cu:1135-1163, read by
+//   invalidateNotFinishedNeighbors at :1921-1928), so for them its output is
+//   undefined; this restatement invalidates them all.
+int orc_knn_query(const float* xyz, int n, const float* q, int nq, int k, float thres_in, int* out,
+                  int* status) {
+    Grid g;
+    build_grid(xyz, n, g, kLevels);
+    float thres = thres_in;
+    thres /= (g.mx - g.mn);
+    thres *= thres;
+    const float d = g.mx - g.mn;
+    int invalid_count = 0;
+#pragma omp parallel reduction(+ : invalid_count)
+    {
+        std::vector<float> dist(k);
+        std::vector<int> idx(k);
+#pragma omp for schedule(dynamic, 256)
+        for (int i = 0; i < nq; i++) {
+            const float x = (q[3 * (size_t)i] - g.mn) / d, y = (q[3 * (size_t)i + 1] - g.mn) / d,
+                        z = (q[3 * (size_t)i + 2] - g.mn) / d;
+            int counter;
+            bool invalid;
+            const int reached = knn_foreign_query(g, x, y, z, k, thres, dist.data(), idx.data(), counter, invalid);
+            if (invalid) invalid_count++;
+            if (status) status[i] = !invalid ? 0 : (reached == kLevels ? 2 : 1);
+            for (int t = 0; t < k; t++) out[(size_t)i * k + t] = idx[t] >= 0 ? g.perm[idx[t]] : -1;
+        }
+    }
     return invalid_count;
 }
 

@@ -34,6 +34,8 @@ def lib():
         L.orc_extents.argtypes = [vp, i32, vp]
         L.orc_knn.restype = i32
         L.orc_knn.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp, vp, vp]
+        L.orc_knn_query.restype = i32
+        L.orc_knn_query.argtypes = [vp, i32, vp, i32, i32, f32, vp, vp]
         L.orc_mesh_1ring.argtypes = [vp, i32, vp, i32, i32, vp, vp, vp, vp]
         L.orc_egt.argtypes = [vp, i32, i32, vp, f32, vp]
         L.orc_taubin_f32.argtypes = [vp, i32, i32, vp, i32, f32, f32]
@@ -75,6 +77,19 @@ def knn(xyz: np.ndarray, k: int):
                         C.byref(visited))
     return dict(lists=lists, pos=pos, perm=perm, ext=ext, level=level, kth=kth, invalid=inv,
                 visited=visited.value)
+
+
+def knn_query(xyz: np.ndarray, queries: np.ndarray, k: int, thres: float = 1e8, with_status: bool = False):
+    """Reference query-vs-reference kNN (GRIDCUDAKNNCompact + GetKNNIndexes):
+    (nq, k) original reference ids in original query order, and the invalid
+    count; with_status adds the per-query status (0 valid, 1 oversized cell,
+    2 still searching after the last level)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+    q = np.ascontiguousarray(queries, dtype=np.float32)
+    out = np.empty((q.shape[0], k), np.int32)
+    st = np.empty(q.shape[0], np.int32)
+    inv = lib().orc_knn_query(_p(xyz), xyz.shape[0], _p(q), q.shape[0], k, float(thres), _p(out), _p(st))
+    return (out, inv, st) if with_status else (out, inv)
 
 
 def mesh_1ring(xyz: np.ndarray, tris: np.ndarray, k: int):

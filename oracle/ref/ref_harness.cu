@@ -14,6 +14,7 @@
 //          -> Normal_CUDA::GetNormals -> getOutputPoints
 //   mesh:  GridMeshCuda(mesh, 1, 1e-6, 1024) -> GetNeighborsFromTriangles(k)
 //          -> PerformSmoothing -> getOutputPoints
+//   query: GridStructure(ref) -> GRIDCUDAKNNCompact(queries) -> GetKNNIndexes
 // The only addition is that every stage is bracketed by cudaEvents and the
 // intermediate device arrays are copied to host buffers supplied by the caller.
 #include <cstdint>
@@ -192,6 +193,33 @@ int egtref_mesh(const float* xyz, int n, const uint32_t* tris, int t, int k, int
         }
     }
     if (stage_ms) for (int i = 0; i < 4; i++) stage_ms[i] = ms[i];
+    return 0;
+}
+
+// Query-vs-reference kNN, the reference's other search (ICP use):
+// GridStructure(ref) -> GRIDCUDAKNNCompact(qx, qy, qz, nq, k, 1e8)
+// (GridKNNCuda.cu:1645-1939) -> GetKNNIndexes (:1941-1968).
+//   q        [nq*3] AoS query points (the reference's units)
+//   knn      [nq*k] original reference ids in original query order
+//   stage_ms [1]    {grid + query kNN}
+int egtref_query(const float* xyz, int n, const float* q, int nq, int k, int* knn, float* stage_ms) {
+    cudaSetDevice(0);
+    Mesh mesh = make_mesh(xyz, n, nullptr, 0);
+    std::vector<float> qx(nq), qy(nq), qz(nq);
+    for (int i = 0; i < nq; i++) {
+        qx[i] = q[3 * (size_t)i];
+        qy[i] = q[3 * (size_t)i + 1];
+        qz[i] = q[3 * (size_t)i + 2];
+    }
+    StageTimer tm;
+    tm.start();
+    auto grid = std::make_shared<GridStructure>(mesh, 1, 1e-6, 1024, 4);
+    grid->GRIDCUDAKNNCompact(qx.data(), qy.data(), qz.data(), nq, k, 1e8);
+    const float ms = tm.stop();
+    if (finish("query knn")) return -1;
+    grid->GetKNNIndexes(knn);
+    if (finish("GetKNNIndexes")) return -1;
+    if (stage_ms) stage_ms[0] = ms;
     return 0;
 }
 

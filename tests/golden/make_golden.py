@@ -45,6 +45,8 @@ def load():
     lib = C.CDLL(LIB)
     lib.egtref_cloud.restype = C.c_int
     lib.egtref_cloud.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int] + [C.c_void_p] * 9
+    lib.egtref_query.restype = C.c_int
+    lib.egtref_query.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
     lib.egtref_mesh.restype = C.c_int
     lib.egtref_mesh.argtypes = ([C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float]
                                 + [C.c_void_p] * 8)
@@ -84,6 +86,30 @@ def run_mesh(lib, xyz, tris, k, iters, alpha):
     if rc != 0:
         raise RuntimeError("reference mesh run failed")
     return o
+
+
+def run_query(lib, xyz, q, k):
+    xyz = np.ascontiguousarray(xyz, np.float32)
+    q = np.ascontiguousarray(q, np.float32)
+    knn = np.empty((q.shape[0], k), np.int32)
+    ms = np.zeros(1, np.float32)
+    rc = lib.egtref_query(_p(xyz), xyz.shape[0], _p(q), q.shape[0], k, _p(knn), _p(ms))
+    if rc != 0:
+        raise RuntimeError("egtref_query failed")
+    return dict(knn=knn, stage_ms=ms)
+
+
+def query_points(xyz, seed):
+    """Queries for the query-vs-reference kNN: jittered reference points (on
+    the surface), uniform points in and around the reference cube (some
+    outside it) and exact copies of reference points (distance 0)."""
+    g = np.random.default_rng(seed)
+    lo, hi = xyz.min(0), xyz.max(0)
+    span = float((hi - lo).max())
+    near = xyz[g.choice(xyz.shape[0], 1500, replace=False)] + g.normal(0, 0.01 * span, (1500, 3))
+    box = lo - 0.15 * span + g.random((800, 3)) * (1.3 * span)
+    same = xyz[g.choice(xyz.shape[0], 200, replace=False)]
+    return np.concatenate([near, box, same]).astype(np.float32)
 
 
 def lattice_cloud(side=16, dup_frac=0.0, seed=21):
@@ -136,10 +162,28 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
     ap.add_argument("--big", action="store_true", help="also run the 4M-point timing case")
+    ap.add_argument("--only-query", action="store_true", help="only the query-vs-reference kNN fixtures")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     lib = load()
     timings = {}
+
+    # query-vs-reference kNN (GRIDCUDAKNNCompact): a noisy sphere and a lattice (ties)
+    xyz = datagen.sphere_cloud(8000, 0.005, 31)
+    q = query_points(xyz, 32)
+    o = run_query(lib, xyz, q, 16)
+    save_full(os.path.join(a.out, "ref_query_sphere.npz"),
+              dict(kind="query", gen="sphere_cloud(8000,0.005,31); query_points(xyz,32)", k=16),
+              {"xyz": xyz, "queries": q}, {"knn": o["knn"]})
+    xyz = lattice_cloud(12)
+    t = np.arange(-2, 14, dtype=np.float32) * np.float32(0.5)
+    q = np.stack(np.meshgrid(t, t, t, indexing="ij"), -1).reshape(-1, 3)[::7].copy()
+    o = run_query(lib, xyz, q, 20)
+    save_full(os.path.join(a.out, "ref_query_lattice.npz"),
+              dict(kind="query", gen="lattice_cloud(12); half-step lattice queries [-1, 6.5]^3 every 7th", k=20),
+              {"xyz": xyz, "queries": q}, {"knn": o["knn"]})
+    if a.only_query:
+        return
 
     # 1. small noisy sphere, full arrays, with normals
     xyz = datagen.sphere_cloud(4096, 0.005, 11)
