@@ -55,7 +55,7 @@ void free_handle(egt_handle* h) {
     F(h->d_counters); F(h->scratch.ptr);
     if (h->taubin_exec) cudaGraphExecDestroy(h->taubin_exec);
     F(h->m_perm); F(h->m_inv); F(h->m_p); F(h->m_pb); F(h->m_off); F(h->m_col);
-    F(h->t_uni); F(h->t_loc); F(h->t_nu);
+    F(h->t_uni); F(h->t_loc); F(h->t_nu); F(h->t_soff);
     cudaStreamSynchronize(h->stream);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);

@@ -177,16 +177,18 @@ struct egt_handle {
     int64_t m_cap = 0;
     // per 256-row tile: distinct neighbour indices (stored at the tile's first
     // CSR offset) and, per CSR entry, its index into that list
-    int* t_uni = nullptr;        // [nnz]
-    uint16_t* t_loc = nullptr;   // [nnz]
-    int* t_nu = nullptr;         // [tiles] distinct count, -1 = tile not staged
+    int* t_uni = nullptr;        // [tiles * 1024] point index of each staged slot
+    uint16_t* t_loc = nullptr;   // [tiles * 5120] slot of each CSR entry, sliced by warp
+    int* t_nu = nullptr;         // [tiles] staged slot count, -1 = tile not staged
+    int* t_soff = nullptr;       // [tiles * 9] slice offsets into t_loc, then the table size
+    int64_t t_tiles = 0;         // tiles the four tables above are sized for
     uint64_t csr_version = 0;    // bumped whenever the CSR is rebuilt
     uint64_t m_version = ~0ull;  // CSR version the Morton copy was built from
     // cached Taubin graph (2*iters half-steps) and the parameters it was built for
     cudaGraphExec_t taubin_exec = nullptr;
     int taubin_iters = -1;
     float taubin_lambda = 0.f, taubin_mu = 0.f;
-    const void* taubin_key[4] = {};
+    const void* taubin_key[8] = {};
     int taubin_mode = 0;         // 0: staged tiles, 1: direct gathers (chosen by the batch autotuner)
     int taubin_graph_mode = -1;  // mode the cached graph was captured with
     // batched clouds: per-point cloud id (sorted order), bits of the largest id

@@ -105,22 +105,15 @@ __device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepco
 __device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;"); }
 
 constexpr int kUCap = 1024;      // distinct neighbours staged per tile (16 KB; 99.8% of tiles fit)
-constexpr int kUPer = kUCap / kTile;  // staged neighbours per thread
-constexpr size_t kStageBytes = kUCap * sizeof(float4) + kTileCap * sizeof(uint16_t);
+constexpr int kUPer = kUCap / kTile;  // staged positions per thread
+constexpr int kSlices = kTile / 32;   // one 32-row slice per warp
+constexpr int kSellCap = 5632;   // neighbour-slot entries per tile, slices padded to their longest row
+constexpr size_t kStageBytes = kUCap * sizeof(float4) + kSellCap * sizeof(uint16_t);
 constexpr int kStages = 2;       // tile buffers per block: one being computed, one being filled
 constexpr size_t kPipeSmem = kStages * kStageBytes;
-static_assert(kTileCap % 8 == 0, "t_loc tiles are copied in 8-entry vectors");
+constexpr int kSoffWords = kSlices + 1;  // per tile: slice offsets and the tile's slot count
+static_assert(kSellCap % 8 == 0, "slot tiles are copied in 8-entry vectors");
 static_assert(kStageBytes % 16 == 0, "stage buffers stay 16-byte aligned");
-
-// First t_loc slot of tile t: its first CSR offset moved up by 8 slots per
-// preceding tile and rounded up to a multiple of 8 (16 bytes).  Consecutive
-// tiles never overlap: base(t+1) >= e_lo(t+1) + 8(t+1) > base(t) + cnt(t).
-__host__ __device__ __forceinline__ int64_t loc_base(int64_t e_lo, int64_t tile) {
-    return (e_lo + 8 * tile + 7) & ~int64_t(7);
-}
-// t_loc length for nnz entries over `tiles` tiles, including the last tile's
-// rounded-up vector.
-inline int64_t loc_slots(int64_t nnz, int64_t tiles) { return nnz + 8 * tiles + 16; }
 
 // 16-byte global -> shared copies that complete asynchronously (cp.async,
 // bypassing L1); commit() closes a group, wait<N>() waits until at most N of
@@ -134,41 +127,42 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // What a thread needs to know about one tile before its data arrive: the
-// tile's CSR range, its distinct-neighbour count, this thread's share of the
-// distinct-neighbour indices and this thread's row range.  Reads only the CSR
-// tables, which no half-step writes.
+// tile's distinct-neighbour count, this thread's share of their point
+// indices, its row's CSR range, and its warp's slice offset and the tile's
+// slot-table size.  Reads only the tile tables, which no half-step writes.
 struct TileRegs {
-    int e_lo, e_hi, nu, e0, e1;
+    int nu, e0, e1, soff, ssize;
     int uni[kUPer];
 };
 
 __device__ __forceinline__ TileRegs tile_regs(const int* __restrict__ off, const int* __restrict__ t_uni,
-                                              const int* __restrict__ t_nu, int tile, int n) {
+                                              const int* __restrict__ t_nu, const int* __restrict__ t_soff,
+                                              int tile, int n) {
     TileRegs r;
-    const int base = tile * kTile, last = min(base + kTile, n), i = base + (int)threadIdx.x;
-    r.e_lo = __ldg(off + base);
-    r.e_hi = __ldg(off + last);
+    const int i = tile * kTile + (int)threadIdx.x;
     r.nu = __ldg(t_nu + tile);
     r.e0 = i < n ? __ldg(off + i) : 0;
     r.e1 = i < n ? __ldg(off + i + 1) : 0;
+    r.soff = r.nu >= 0 ? __ldg(t_soff + (size_t)tile * kSoffWords + (threadIdx.x >> 5)) : 0;
+    r.ssize = r.nu >= 0 ? __ldg(t_soff + (size_t)tile * kSoffWords + kSlices) : 0;
 #pragma unroll
     for (int u = 0; u < kUPer; u++) {
         const int j = (int)threadIdx.x + u * kTile;
-        r.uni[u] = (r.nu >= 0 && j < r.nu) ? __ldg(t_uni + r.e_lo + j) : 0;
+        r.uni[u] = (r.nu >= 0 && j < r.nu) ? __ldg(t_uni + (size_t)tile * kUCap + j) : 0;
     }
     return r;
 }
 
 // Starts the copies of one tile into a stage buffer: the tile's 16-bit
-// neighbour slots (contiguous, 16-byte aligned) and its distinct neighbour
+// neighbour slots (a fixed-stride, 16-byte aligned table) and its staged
 // positions (one 16-byte gather each).  Always commits one group.
 __device__ __forceinline__ void tile_fetch(const TileRegs& r, const float4* __restrict__ pin,
                                            const uint16_t* __restrict__ t_loc, int tile, unsigned char* stage) {
     if (r.nu >= 0) {
         float4* s_pos = reinterpret_cast<float4*>(stage);
         uint16_t* s_loc = reinterpret_cast<uint16_t*>(stage + kUCap * sizeof(float4));
-        const uint16_t* src = t_loc + loc_base(r.e_lo, tile);
-        const int nvec = (r.e_hi - r.e_lo + 7) >> 3;
+        const uint16_t* src = t_loc + (size_t)tile * kSellCap;
+        const int nvec = (r.ssize + 7) >> 3;
         for (int v = (int)threadIdx.x; v < nvec; v += kTile) cp_async16(s_loc + 8 * v, src + 8 * v);
 #pragma unroll
         for (int u = 0; u < kUPer; u++) {
@@ -180,29 +174,33 @@ __device__ __forceinline__ void tile_fetch(const TileRegs& r, const float4* __re
 }
 
 // Staged half-step, persistent and double-buffered.  Every kTile-row tile
-// has its distinct neighbour indices (t_uni, precomputed once per CSR) and,
-// per CSR entry, a 16-bit index into that list (t_loc).  Block b takes tiles
-// b, b + gridDim.x, ...; while it computes one tile from shared memory, the
-// copies of its next tile are in flight into the other buffer, and the
-// registers for the tile after that are being loaded.  Each distinct
-// neighbour position is fetched from global memory once per tile, and rows
-// read their neighbours from shared memory in list order.  Tiles whose lists
-// do not fit (t_nu < 0) gather from global memory directly.  Within a tile the
-// rows are ordered by decreasing neighbour count (see morton_prepare), so
-// the 32 rows of a warp walk rows of nearly equal length.
+// has its staged neighbour positions (t_uni: point index of each position
+// slot, precomputed once per CSR) and, per CSR entry, the 16-bit slot of its
+// neighbour (t_loc).  Block b takes tiles b, b + gridDim.x, ...; while it
+// computes one tile from shared memory, the copies of its next tile are in
+// flight into the other buffer, and the registers for the tile after that
+// are being loaded.  Each distinct neighbour position is fetched from global
+// memory once per tile; each row reads its neighbours from shared memory in
+// list order.  Tiles that do not fit (t_nu < 0) gather from global memory.
+//
+// The slots are sliced: warp w's 32 rows (ordered by decreasing neighbour
+// count, see morton_prepare) store entry e of lane l at soff[w] + 32 e + l, so
+// each step of a warp reads 64 contiguous bytes of slots.
 __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restrict__ pin, float4* __restrict__ pout,
                                                         const int* __restrict__ off, const int* __restrict__ col,
                                                         const int* __restrict__ t_uni,
                                                         const uint16_t* __restrict__ t_loc,
-                                                        const int* __restrict__ t_nu, int n, int tiles, float scale) {
+                                                        const int* __restrict__ t_nu, const int* __restrict__ t_soff,
+                                                        int n, int tiles, float scale) {
     extern __shared__ __align__(16) unsigned char smem[];
     int tile = blockIdx.x;
     if (tile >= tiles) return;
-    // Before grid_dependency_wait() only the CSR tables are read: under
+    const int lane = threadIdx.x & 31;
+    // Before grid_dependency_wait() only the tile tables are read: under
     // programmatic dependent launch this overlaps the previous half-step.
-    TileRegs cur = tile_regs(off, t_uni, t_nu, tile, n);
+    TileRegs cur = tile_regs(off, t_uni, t_nu, t_soff, tile, n);
     int next = tile + gridDim.x;
-    TileRegs nxt = next < tiles ? tile_regs(off, t_uni, t_nu, next, n) : cur;
+    TileRegs nxt = next < tiles ? tile_regs(off, t_uni, t_nu, t_soff, next, n) : cur;
     grid_dependency_wait();  // the previous half-step's positions are complete
     grid_dependents_launch();
     tile_fetch(cur, pin, t_loc, tile, smem);
@@ -220,7 +218,7 @@ __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restr
             cp_async_commit();  // keep one group per round
         }
         const int after = next + (int)gridDim.x;
-        const TileRegs nn = after < tiles ? tile_regs(off, t_uni, t_nu, after, n) : nxt;
+        const TileRegs nn = after < tiles ? tile_regs(off, t_uni, t_nu, t_soff, after, n) : nxt;
         cp_async_wait<1>();  // this thread's copies of the current tile have landed
         __syncthreads();     // ... and everyone else's
         if (i < n) {
@@ -230,10 +228,26 @@ __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restr
                     accumulate(p.x, p.y, p.z, __ldg(pin + __ldg(col + e)), cx, cy, cz, sum);
             } else {
                 const float4* s_pos = reinterpret_cast<const float4*>(stage);
-                const uint16_t* s_loc = reinterpret_cast<const uint16_t*>(stage + kUCap * sizeof(float4));
-                const int e0 = cur.e0 - cur.e_lo, e1 = cur.e1 - cur.e_lo;
-#pragma unroll 4
-                for (int e = e0; e < e1; e++) accumulate(p.x, p.y, p.z, s_pos[s_loc[e]], cx, cy, cz, sum);
+                const uint2* ls =
+                    reinterpret_cast<const uint2*>(stage + kUCap * sizeof(float4) + 2 * cur.soff) + lane;
+                const int len = cur.e1 - cur.e0;
+                int e = 0;
+#pragma unroll 2
+                for (; e + 4 <= len; e += 4) {
+                    const uint2 v = ls[8 * e];
+                    const float4 q0 = s_pos[v.x & 0xffff], q1 = s_pos[v.x >> 16];
+                    const float4 q2 = s_pos[v.y & 0xffff], q3 = s_pos[v.y >> 16];
+                    accumulate(p.x, p.y, p.z, q0, cx, cy, cz, sum);
+                    accumulate(p.x, p.y, p.z, q1, cx, cy, cz, sum);
+                    accumulate(p.x, p.y, p.z, q2, cx, cy, cz, sum);
+                    accumulate(p.x, p.y, p.z, q3, cx, cy, cz, sum);
+                }
+                if (e < len) {
+                    const uint2 v = ls[8 * e];
+                    accumulate(p.x, p.y, p.z, s_pos[v.x & 0xffff], cx, cy, cz, sum);
+                    if (e + 1 < len) accumulate(p.x, p.y, p.z, s_pos[v.x >> 16], cx, cy, cz, sum);
+                    if (e + 2 < len) accumulate(p.x, p.y, p.z, s_pos[v.y & 0xffff], cx, cy, cz, sum);
+                }
             }
             pout[i] = finish(p, cx, cy, cz, sum, scale);
         }
@@ -248,14 +262,21 @@ __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restr
     cp_async_wait<0>();
 }
 
-// Builds t_uni / t_loc / t_nu for one tile: block radix sort of the tile's
-// column indices, unique, then each entry's position in the unique list.
+// Builds the tables of one tile (one block per tile): a block radix sort of
+// the tile's column indices and a unique pass give the distinct neighbours
+// (t_uni, at a fixed stride of kUCap per tile) and each CSR entry's index
+// into them, a 16-bit slot; the slots are stored sliced by warp (warp w's 32
+// rows padded to its longest row, entry e of lane l at soff[w] + 32 e + l,
+// t_soff = soff[0..8] with soff[8] the table size).  t_nu = the distinct
+// count, or -1 when the tile does not fit (too many entries, distinct
+// neighbours or padded slots): its rows then gather from global memory.
 constexpr int kBuildThreads = 512;
 constexpr int kBuildItems = kTileCap / kBuildThreads;
 
 __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restrict__ off, const int* __restrict__ col,
                                                               int n, int* __restrict__ t_uni,
-                                                              uint16_t* __restrict__ t_loc, int* __restrict__ t_nu) {
+                                                              uint16_t* __restrict__ t_loc, int* __restrict__ t_nu,
+                                                              int* __restrict__ t_soff) {
     using Sort = cub::BlockRadixSort<int, kBuildThreads, kBuildItems>;
     using Scan = cub::BlockScan<int, kBuildThreads>;
     __shared__ union {
@@ -264,13 +285,18 @@ __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restr
     } sm;
     __shared__ typename Scan::TempStorage scan;
     __shared__ int s_last[kBuildThreads];
+    __shared__ uint16_t s_u[kTileCap];  // entry -> distinct index
+    __shared__ int s_len[kTile], s_start[kTile];
+    __shared__ int s_soff[kSoffWords];
     __shared__ int s_nu;
-    const int base = blockIdx.x * kTile;
+    const int tile = blockIdx.x;
+    const int base = tile * kTile;
     const int last = min(base + kTile, n);
+    const int rows = last - base;
     const int e_lo = off[base], e_hi = off[last];
     const int cnt = e_hi - e_lo;
     if (cnt > kTileCap) {
-        if (threadIdx.x == 0) t_nu[blockIdx.x] = -1;
+        if (threadIdx.x == 0) t_nu[tile] = -1;
         return;
     }
     int keys[kBuildItems];
@@ -298,13 +324,16 @@ __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restr
     for (int j = 0; j < kBuildItems; j++)
         if (first[j]) sm.uniq[at++] = keys[j];
     if (threadIdx.x == 0) s_nu = total;
+    for (int r = threadIdx.x; r < kTile; r += kBuildThreads) {
+        s_len[r] = r < rows ? off[base + r + 1] - off[base + r] : 0;
+        s_start[r] = r < rows ? off[base + r] - e_lo : 0;
+    }
     __syncthreads();
     const int nu = s_nu;
     if (nu > kUCap) {
-        if (threadIdx.x == 0) t_nu[blockIdx.x] = -1;
+        if (threadIdx.x == 0) t_nu[tile] = -1;
         return;
     }
-    for (int u = threadIdx.x; u < nu; u += kBuildThreads) t_uni[e_lo + u] = sm.uniq[u];
     for (int i = threadIdx.x; i < cnt; i += kBuildThreads) {
         const int v = col[e_lo + i];
         int lo = 0, hi = nu - 1;
@@ -313,9 +342,31 @@ __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restr
             if (sm.uniq[mid] < v) lo = mid + 1;
             else hi = mid;
         }
-        t_loc[loc_base(e_lo, blockIdx.x) + i] = (uint16_t)lo;
+        s_u[i] = (uint16_t)lo;
     }
-    if (threadIdx.x == 0) t_nu[blockIdx.x] = nu;
+    if (threadIdx.x == 0) {
+        s_soff[0] = 0;
+        for (int w = 0; w < kSlices; w++) {
+            int wmax = 0;
+            for (int l = 0; l < 32; l++) wmax = max(wmax, s_len[32 * w + l]);
+            s_soff[w + 1] = s_soff[w] + 32 * ((wmax + 3) & ~3);
+        }
+    }
+    __syncthreads();
+    if (s_soff[kSlices] > kSellCap) {
+        if (threadIdx.x == 0) t_nu[tile] = -1;
+        return;
+    }
+    for (int u = threadIdx.x; u < nu; u += kBuildThreads) t_uni[(size_t)tile * kUCap + u] = sm.uniq[u];
+    const int ssize = s_soff[kSlices];
+    for (int x = threadIdx.x; x < ssize; x += kBuildThreads) {
+        int w = 0;
+        while (x >= s_soff[w + 1]) w++;
+        const int rel = x - s_soff[w], e = 4 * (rel >> 7) + (rel & 3), r = 32 * w + ((rel >> 2) & 31);
+        t_loc[(size_t)tile * kSellCap + x] = e < s_len[r] ? s_u[s_start[r] + e] : (uint16_t)0;
+    }
+    if (threadIdx.x < kSoffWords) t_soff[(size_t)tile * kSoffWords + threadIdx.x] = s_soff[threadIdx.x];
+    if (threadIdx.x == 0) t_nu[tile] = nu;
 }
 
 __global__ void k_split_soa(const float4* __restrict__ p4, int n, float* __restrict__ x, float* __restrict__ y,
@@ -432,8 +483,8 @@ static egt_status staged_launch(egt_handle* h, const float4* pin, float4* pout, 
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     EGT_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_taubin_tiles, pin, pout, (const int*)h->m_off, (const int*)h->m_col,
-                                    (const int*)h->t_uni, (const uint16_t*)h->t_loc, (const int*)h->t_nu, n, tiles,
-                                    scale));
+                                    (const int*)h->t_uni, (const uint16_t*)h->t_loc, (const int*)h->t_nu,
+                                    (const int*)h->t_soff, n, tiles, scale));
     EGT_LAUNCH_CHECK();
     return EGT_OK;
 }
@@ -505,15 +556,23 @@ static egt_status morton_prepare(egt_handle* h) {
         EGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, t_scan, len, h->m_off, n + 1, st));
         k_morton_cols<<<G, 256, 0, st>>>(h->m_perm, h->m_inv, h->csr_off, h->csr_col, h->m_off, n, h->m_col);
         EGT_LAUNCH_CHECK();
-        // per-tile distinct-neighbour lists for the staged half-step
-        if (h->t_uni) dev_free(h, h->t_uni);
-        if (h->t_loc) dev_free(h, h->t_loc);
-        if (h->t_nu) dev_free(h, h->t_nu);
-        h->t_uni = nullptr; h->t_loc = nullptr; h->t_nu = nullptr;
-        EGT_CUDA_TRY(dev_alloc(h, &h->t_uni, sizeof(int) * std::max<int64_t>(nnz, 1)));
-        EGT_CUDA_TRY(dev_alloc(h, &h->t_loc, sizeof(uint16_t) * loc_slots(nnz, tiles)));
-        EGT_CUDA_TRY(dev_alloc(h, &h->t_nu, sizeof(int) * tiles));
-        k_tile_build<<<(unsigned)tiles, kBuildThreads, 0, st>>>(h->m_off, h->m_col, n, h->t_uni, h->t_loc, h->t_nu);
+        // per-tile staged-slot tables for the staged half-step (fixed strides
+        // per tile; the sizes depend only on n, so they are kept across CSRs)
+        if (h->t_tiles != tiles) {
+            if (h->t_uni) dev_free(h, h->t_uni);
+            if (h->t_loc) dev_free(h, h->t_loc);
+            if (h->t_nu) dev_free(h, h->t_nu);
+            if (h->t_soff) dev_free(h, h->t_soff);
+            h->t_uni = nullptr; h->t_loc = nullptr; h->t_nu = nullptr; h->t_soff = nullptr;
+            h->t_tiles = 0;
+            EGT_CUDA_TRY(dev_alloc(h, &h->t_uni, sizeof(int) * kUCap * tiles));
+            EGT_CUDA_TRY(dev_alloc(h, &h->t_loc, sizeof(uint16_t) * kSellCap * tiles));
+            EGT_CUDA_TRY(dev_alloc(h, &h->t_nu, sizeof(int) * tiles));
+            EGT_CUDA_TRY(dev_alloc(h, &h->t_soff, sizeof(int) * kSoffWords * tiles));
+            h->t_tiles = tiles;
+        }
+        k_tile_build<<<(unsigned)tiles, kBuildThreads, 0, st>>>(h->m_off, h->m_col, n, h->t_uni, h->t_loc, h->t_nu,
+                                                                 h->t_soff);
         EGT_LAUNCH_CHECK();
         cudaFreeAsync(kin, st);
         cudaFreeAsync(kout, st);
@@ -555,10 +614,11 @@ egt_status run_taubin(egt_handle* h, int iters, float lambda, float mu) {
             attr_set.fetch_or(uint64_t(1) << (dev & 63));
         }
         const unsigned blocks = wave[dev & 63].load();
-        const void* key[4] = {h->m_p, h->m_pb, h->t_uni, h->t_loc};
+        // every buffer the captured launches name
+        const void* key[8] = {h->m_p, h->m_pb, h->t_uni, h->t_loc, h->t_nu, h->t_soff, h->m_off, h->m_col};
         const bool reuse = h->taubin_exec && h->taubin_iters == iters && h->taubin_lambda == lambda &&
                            h->taubin_mu == mu && h->taubin_graph_mode == h->taubin_mode &&
-                           std::equal(key, key + 4, h->taubin_key);
+                           std::equal(key, key + 8, h->taubin_key);
         if (!reuse) {
             if (h->taubin_exec) { cudaGraphExecDestroy(h->taubin_exec); h->taubin_exec = nullptr; }
             // capture the 2*iters half-steps once; replays reuse the executable graph
@@ -598,7 +658,7 @@ egt_status run_taubin(egt_handle* h, int iters, float lambda, float mu) {
             h->taubin_graph_mode = h->taubin_mode;
             h->taubin_lambda = lambda;
             h->taubin_mu = mu;
-            std::copy(key, key + 4, h->taubin_key);
+            std::copy(key, key + 8, h->taubin_key);
         } else {
             // the graph's launches are counted at capture; count the replayed ones too
             for (int i = 0; i < 2 * iters; i++) count_launch();
