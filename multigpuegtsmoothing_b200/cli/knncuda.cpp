@@ -8,8 +8,12 @@
 // prints "Succeeded!".  lambda = 0.63 and mu = -0.64 as in main.cpp:116.
 // This build runs on one GPU: ncards must be 1.
 //
+// With EGT_CLI_TIMING set in the environment, the wall-clock time of the PLY
+// read, the pipeline and the PLY write is printed to stderr.
+//
 // Extra mode used by the tests (no GPU needed):
 //   KNNCUDA --ply-roundtrip in.ply out.ply
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -50,6 +54,8 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "KNNCUDA: this build runs on one GPU; ncards must be 1\n");
         return 1;
     }
+    using clock = std::chrono::steady_clock;
+    const auto t_read = clock::now();
     ply::Mesh mesh;
     std::string err;
     if (!ply::read(path, mesh, err)) {
@@ -57,6 +63,7 @@ int main(int argc, char** argv) {
         return 1;
     }
     const size_t n = mesh.nV();
+    const auto t_pipe = clock::now();
     try {
         using namespace egtb200;
         std::vector<float> ox(n), oy(n), oz(n), nx(n), ny(n), nz(n);
@@ -87,9 +94,17 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "KNNCUDA: %s\n", e.what());
         return 1;
     }
+    const auto t_write = clock::now();
     if (!ply::write("output.ply", mesh, err)) {
         std::fprintf(stderr, "KNNCUDA: %s\n", err.c_str());
         return 1;
+    }
+    if (std::getenv("EGT_CLI_TIMING")) {
+        auto ms = [](clock::time_point a, clock::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        std::fprintf(stderr, "KNNCUDA timing: points %zu read_ms %.1f pipeline_ms %.1f write_ms %.1f\n", n,
+                     ms(t_read, t_pipe), ms(t_pipe, t_write), ms(t_write, clock::now()));
     }
     std::printf("Succeeded!\n");
     return 0;

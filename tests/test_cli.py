@@ -85,6 +85,86 @@ def test_ply_roundtrip(tmp_path, ascii, big):
     assert np.array_equal(F, tris)
 
 
+@pytest.mark.parametrize("layout", ["le_float", "be_double", "ascii_lines", "ascii_split", "quads"])
+def test_ply_large_inputs(tmp_path, layout):
+    """Inputs large enough for the parallel decoders (fixed-size binary
+    records, one ASCII record per line, all-triangle face lists), and the
+    layouts that fall back to the sequential reader (records split over
+    lines, polygons other than triangles); every one must read the same
+    values."""
+    rng = np.random.default_rng(7)
+    n, nf = 200_003, 150_001
+    xyz = rng.normal(size=(n, 3)) * 50.0
+    rgb = rng.integers(0, 256, (n, 3))
+    tris = rng.integers(0, n, (nf, 3))
+    src = tmp_path / "big.ply"
+    if layout == "le_float":
+        xyz = xyz.astype(np.float32).astype(np.float64)
+        hdr = (f"ply\nformat binary_little_endian 1.0\nelement vertex {n}\nproperty float x\nproperty float y\n"
+               f"property float z\nproperty uchar red\nproperty uchar green\nproperty uchar blue\n"
+               f"element face {nf}\nproperty list uchar int vertex_indices\nend_header\n")
+        rec = np.zeros(n, dtype=[("p", "<f4", 3), ("c", "u1", 3)])
+        rec["p"] = xyz
+        rec["c"] = rgb
+        frec = np.zeros(nf, dtype=[("k", "u1"), ("i", "<i4", 3)])
+        frec["k"] = 3
+        frec["i"] = tris
+        src.write_bytes(hdr.encode() + rec.tobytes() + frec.tobytes())
+    elif layout in ("be_double", "quads"):
+        hdr = (f"ply\nformat binary_big_endian 1.0\nelement vertex {n}\nproperty double x\nproperty short s\n"
+               f"property double y\nproperty double z\nproperty uchar red\nproperty uchar green\n"
+               f"property uchar blue\nelement face {nf}\nproperty list uchar uint vertex_indices\nend_header\n")
+        rec = np.zeros(n, dtype=[("x", ">f8"), ("s", ">i2"), ("y", ">f8"), ("z", ">f8"), ("c", "u1", 3)])
+        rec["x"], rec["y"], rec["z"] = xyz[:, 0], xyz[:, 1], xyz[:, 2]
+        rec["c"] = rgb
+        if layout == "be_double":
+            frec = np.zeros(nf, dtype=[("k", "u1"), ("i", ">u4", 3)])
+            frec["k"] = 3
+            frec["i"] = tris
+            body = frec.tobytes()
+        else:  # every fifth face is a quad: its first three indices are kept
+            parts = []
+            for j, t in enumerate(tris):
+                if j % 5 == 0:
+                    parts.append(struct.pack(">B4I", 4, *map(int, t), 0))
+                else:
+                    parts.append(struct.pack(">B3I", 3, *map(int, t)))
+            body = b"".join(parts)
+        src.write_bytes(hdr.encode() + rec.tobytes() + body)
+    else:
+        hdr = (f"ply\nformat ascii 1.0\ncomment generated\nelement vertex {n}\nproperty double x\n"
+               f"property double y\nproperty double z\nproperty uchar red\nproperty uchar green\n"
+               f"property uchar blue\nelement face {nf}\nproperty list uchar int vertex_indices\nend_header\n")
+        lines = [f"{a!r} {b!r} {c!r} {r} {g} {bb}" for (a, b, c), (r, g, bb) in zip(xyz.tolist(), rgb.tolist())]
+        if layout == "ascii_split":  # a record spread over two lines
+            lines[n // 2] = lines[n // 2].replace(" ", "\n", 1)
+        faces = [f"3 {a} {b} {c}" for a, b, c in tris.tolist()]
+        src.write_bytes((hdr + "\n".join(lines) + "\n" + "\n".join(faces) + "\n").encode())
+    dst = tmp_path / "out.ply"
+    subprocess.run([BIN, "--ply-roundtrip", str(src), str(dst)], check=True)
+    data = dst.read_bytes()
+    end = data.index(b"end_header\n") + len(b"end_header\n")
+    out = np.frombuffer(data, dtype=[("p", "<f4", 3), ("c", "u1", 3)], count=n, offset=end)
+    assert np.array_equal(out["p"], xyz.astype(np.float32))
+    assert np.array_equal(out["c"].astype(np.int64), rgb)
+    fo = np.frombuffer(data, dtype=[("k", "u1"), ("i", "<u4", 3)], count=nf, offset=end + n * 15)
+    assert np.all(fo["k"] == 3)
+    assert np.array_equal(fo["i"].astype(np.int64), tris)
+
+
+def test_ply_rejects_truncated_data(tmp_path):
+    n = 100_000
+    hdr = (f"ply\nformat binary_little_endian 1.0\nelement vertex {n}\nproperty float x\nproperty float y\n"
+           f"property float z\nelement face 10\nproperty list uchar int vertex_indices\nend_header\n").encode()
+    body = np.zeros(3 * n, np.float32).tobytes() + b"".join(struct.pack("<B3i", 3, 0, 1, 2) for _ in range(10))
+    for cut, what in [(len(hdr) - 5, b"end_header"), (len(hdr) + 1000, b"truncated vertex"),
+                      (len(hdr) + len(body) - 1, b"truncated face")]:
+        src = tmp_path / "cut.ply"
+        src.write_bytes((hdr + body)[:cut])
+        r = subprocess.run([BIN, "--ply-roundtrip", str(src), str(tmp_path / "o.ply")], capture_output=True)
+        assert r.returncode != 0 and what in r.stderr, (cut, r.stderr)
+
+
 def test_cli_rejects_bad_arguments(tmp_path):
     r = subprocess.run([BIN], capture_output=True)
     assert r.returncode != 0 and b"usage" in r.stderr
