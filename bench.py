@@ -84,21 +84,79 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 10 ms from a background thread (the region can
+    be shorter than nvidia-smi's 200 ms loop), nvidia-smi when NVML is absent.
+    Reads only; changes no setting."""
+
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
+        import threading
+        self.sm, self.smax, self.reasons = [], [], set()
+        self.p = None
+        self.thread = None
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        nvml_index = int(ids[index]) if index < len(ids) and ids[index].isdigit() else index
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(nvml_index)
+            self.masks = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                          pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
+        except Exception:
+            self.nvml = None
+        if self.nvml is not None:
+            self.stop_flag = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}",
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(nvml_index), f"--query-gpu={q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
 
+    def _sample(self):
+        nv = self.nvml
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+        self.smax.append(float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)))
+        active = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        for nm, m in zip(self.NAMES, self.masks):
+            if active & m:
+                self.reasons.add(nm)
+
+    def _poll(self):
+        while True:
+            try:
+                self._sample()
+            except Exception:
+                return
+            if self.stop_flag.wait(0.01):
+                return
+
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join()
+            try:
+                self._sample()  # at least one sample at the end of the region
+            except Exception:
+                pass
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+            return {"sm_mhz": statistics.median(self.sm) if self.sm else None,
+                    "sm_max_mhz": max(self.smax) if self.smax else None,
+                    "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvml, 10 ms"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -109,19 +167,18 @@ class ClockSampler:
         self.f.flush()
         rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
         os.unlink(self.f.name)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             try:
-                sm.append(float(r[1]))
-                smax.append(float(r[2]))
-                for nm, v in zip(names, r[5:9]):
+                self.sm.append(float(r[1]))
+                self.smax.append(float(r[2]))
+                for nm, v in zip(self.NAMES, r[5:9]):
                     if v.strip().lower() == "active":
-                        reasons.add(nm)
+                        self.reasons.add(nm)
             except (ValueError, IndexError):
                 continue
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None,
+                "sm_max_mhz": max(self.smax) if self.smax else None,
+                "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvidia-smi, 200 ms"}
 
 
 def dist_setup(init: bool = True):
