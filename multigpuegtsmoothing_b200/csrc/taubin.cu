@@ -231,19 +231,22 @@ __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restr
                 const uint2* ls =
                     reinterpret_cast<const uint2*>(stage + kUCap * sizeof(float4) + 2 * cur.soff) + lane;
                 const int len = cur.e1 - cur.e0;
+                // four neighbours per step; the next step's slot word is loaded
+                // before this step's positions are read, off the critical path
                 int e = 0;
-#pragma unroll 2
+                uint2 v = len > 0 ? ls[0] : make_uint2(0u, 0u);
+#pragma unroll 1
                 for (; e + 4 <= len; e += 4) {
-                    const uint2 v = ls[8 * e];
+                    const uint2 vn = e + 4 < len ? ls[8 * (e + 4)] : v;
                     const float4 q0 = s_pos[v.x & 0xffff], q1 = s_pos[v.x >> 16];
                     const float4 q2 = s_pos[v.y & 0xffff], q3 = s_pos[v.y >> 16];
                     accumulate(p.x, p.y, p.z, q0, cx, cy, cz, sum);
                     accumulate(p.x, p.y, p.z, q1, cx, cy, cz, sum);
                     accumulate(p.x, p.y, p.z, q2, cx, cy, cz, sum);
                     accumulate(p.x, p.y, p.z, q3, cx, cy, cz, sum);
+                    v = vn;
                 }
                 if (e < len) {
-                    const uint2 v = ls[8 * e];
                     accumulate(p.x, p.y, p.z, s_pos[v.x & 0xffff], cx, cy, cz, sum);
                     if (e + 1 < len) accumulate(p.x, p.y, p.z, s_pos[v.x >> 16], cx, cy, cz, sum);
                     if (e + 2 < len) accumulate(p.x, p.y, p.z, s_pos[v.y & 0xffff], cx, cy, cz, sum);
