@@ -183,9 +183,10 @@ __device__ __forceinline__ void tile_fetch(const TileRegs& r, const float4* __re
 // memory once per tile; each row reads its neighbours from shared memory in
 // list order.  Tiles that do not fit (t_nu < 0) gather from global memory.
 //
-// The slots are sliced: warp w's 32 rows (ordered by decreasing neighbour
-// count, see morton_prepare) store entry e of lane l at soff[w] + 32 e + l, so
-// each step of a warp reads 64 contiguous bytes of slots.
+// The slots are sliced in groups of four: warp w's 32 rows (ordered by
+// decreasing neighbour count, see morton_prepare) store entries 4g..4g+3 of
+// lane l at soff[w] + 128 g + 4 l, so each step of a warp (four neighbours per
+// lane) reads 256 contiguous bytes of slots.
 __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restrict__ pin, float4* __restrict__ pout,
                                                         const int* __restrict__ off, const int* __restrict__ col,
                                                         const int* __restrict__ t_uni,
@@ -208,19 +209,19 @@ __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restr
     float4 p = i < n ? __ldg(pin + i) : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int j = 0; tile < tiles; j++) {
         unsigned char* stage = smem + (j & 1) * kStageBytes;
-        // the next tile's copies go to the buffer computed in the previous round
+        cp_async_wait<0>();  // this thread's copies of the current tile have landed
+        // One barrier per tile: past it, every thread's copies of the current
+        // tile are visible, and every thread has finished the previous tile,
+        // so the other buffer is free for the next tile's copies.
+        __syncthreads();
         float4 p_next = p;
         if (next < tiles) {
             tile_fetch(nxt, pin, t_loc, next, smem + ((j + 1) & 1) * kStageBytes);
             const int in = next * kTile + (int)threadIdx.x;
             if (in < n) p_next = __ldg(pin + in);
-        } else {
-            cp_async_commit();  // keep one group per round
         }
         const int after = next + (int)gridDim.x;
         const TileRegs nn = after < tiles ? tile_regs(off, t_uni, t_nu, t_soff, after, n) : nxt;
-        cp_async_wait<1>();  // this thread's copies of the current tile have landed
-        __syncthreads();     // ... and everyone else's
         if (i < n) {
             float cx = 0.0f, cy = 0.0f, cz = 0.0f, sum = 0.0f;
             if (cur.nu < 0) {  // tile too large to stage: plain gathers
@@ -254,7 +255,6 @@ __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restr
             }
             pout[i] = finish(p, cx, cy, cz, sum, scale);
         }
-        __syncthreads();  // the buffer is free for the tile after next
         tile = next;
         next = after;
         cur = nxt;
@@ -269,8 +269,9 @@ __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restr
 // the tile's column indices and a unique pass give the distinct neighbours
 // (t_uni, at a fixed stride of kUCap per tile) and each CSR entry's index
 // into them, a 16-bit slot; the slots are stored sliced by warp (warp w's 32
-// rows padded to its longest row, entry e of lane l at soff[w] + 32 e + l,
-// t_soff = soff[0..8] with soff[8] the table size).  t_nu = the distinct
+// rows padded to its longest row rounded up to 4, entry 4g + r of lane l at
+// soff[w] + 128 g + 4 l + r, t_soff = soff[0..8] with soff[8] the table
+// size).  t_nu = the distinct
 // count, or -1 when the tile does not fit (too many entries, distinct
 // neighbours or padded slots): its rows then gather from global memory.
 constexpr int kBuildThreads = 512;
