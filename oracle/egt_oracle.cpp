@@ -21,6 +21,7 @@
 #include <numeric>
 #include <queue>
 #include <set>
+#include <unordered_set>
 #include <vector>
 #include <omp.h>
 
@@ -1191,6 +1192,85 @@ int orc_orient(int n, int k, const int* lists, float* nrm, int* parent) {
     return ncomp;
 }
 
+// The reference's CPU orienter orient_kruskal (MST.cpp:399-423) with
+// Graph::kruskalMST (:297-376), DisjointSets (:185-229) and
+// orientSpanningTree (:262-279), in place on host normals.
+//   * Edges: for every row i and its first k_use entries m >= 0, the pair
+//     (min, max) is kept at its first occurrence (keyed u*n+v; the reference
+//     forms that key in 32-bit int arithmetic, which overflows above 46,340
+//     points -- this restatement uses 64 bits, the evident intent).  Weight =
+//     max(0, 1 - |d|) in double, d the float dot product
+//     nx_i*nx_m + ny_i*ny_m + nz_i*nz_m evaluated left to right without
+//     fusion.
+//   * Kruskal over the edges sorted by (weight, u, v), with a union-find that
+//     merges by rank (the second root wins ties and gains a rank) and
+//     compresses paths; accepted edges are appended to both endpoints'
+//     adjacency lists.
+//   * Every union-find root r (parent[r] == r, scanned in index order) starts
+//     a depth-first walk with an explicit stack: pop u, then for each
+//     unprocessed neighbour v in adjacency order negate n_v when the float
+//     dot product of n_u and n_v is negative and push v; u is then processed.
+void orient_kruskal_impl(const int* knn, int64_t n, int k, int k_use, float* nx, float* ny, float* nz) {
+    struct Edge { double w; int u, v; };
+    auto dotf = [&](int a, int b) {
+        const float t = nx[a] * nx[b] + ny[a] * ny[b];
+        return t + nz[a] * nz[b];
+    };
+    std::vector<Edge> edges;
+    std::unordered_set<uint64_t> seen;
+    seen.reserve((size_t)n * (size_t)std::max(1, k_use));
+    for (int64_t i = 0; i < n; i++)
+        for (int j = 0; j < k_use; j++) {
+            const int m = knn[i * k + j];
+            if (m < 0) continue;
+            const int u = (int)std::min<int64_t>(i, m), v = (int)std::max<int64_t>(i, m);
+            if (!seen.insert((uint64_t)u * (uint64_t)n + (uint64_t)v).second) continue;
+            const double d = (double)dotf((int)i, m);
+            const double w = std::max(0.0, 1.0 - std::fabs(d));
+            edges.push_back({w, u, v});
+        }
+    std::sort(edges.begin(), edges.end(), [](const Edge& a, const Edge& b) {
+        if (a.w != b.w) return a.w < b.w;
+        if (a.u != b.u) return a.u < b.u;
+        return a.v < b.v;
+    });
+    std::vector<int> par((size_t)n + 1), rnk((size_t)n + 1, 0);
+    std::iota(par.begin(), par.end(), 0);
+    auto find = [&](int x) {
+        int r = x;
+        while (par[r] != r) r = par[r];
+        while (par[x] != r) { const int nx_ = par[x]; par[x] = r; x = nx_; }
+        return r;
+    };
+    std::vector<std::vector<int>> adj((size_t)n);
+    for (const Edge& e : edges) {
+        const int a = find(e.u), b = find(e.v);
+        if (a == b) continue;
+        adj[e.v].push_back(e.u);
+        adj[e.u].push_back(e.v);
+        if (rnk[a] > rnk[b]) par[b] = a;
+        else par[a] = b;
+        if (rnk[a] == rnk[b]) rnk[b]++;
+    }
+    std::vector<char> processed((size_t)n, 0);
+    std::vector<int> stack;
+    for (int64_t r = 0; r < n; r++) {
+        if (par[r] != r) continue;
+        stack.push_back((int)r);
+        while (!stack.empty()) {
+            const int u = stack.back();
+            stack.pop_back();
+            for (int v : adj[u]) {
+                if (processed[v]) continue;
+                if (dotf(u, v) < 0) { nx[v] = -nx[v]; ny[v] = -ny[v]; nz[v] = -nz[v]; }
+                stack.push_back(v);
+            }
+            processed[u] = 1;
+        }
+    }
+}
+
+
 // getOutputPoints (getOutputPoints.cu:9-63): denormalise and scatter to the
 // original order.  pos [3n] sorted SoA -> out [3n] original-order SoA.
 void orc_output(const float* pos, const int* perm, const float* ext, int n, float* out) {
@@ -1225,6 +1305,11 @@ void orc_bruteforce(const float* pos, int n, int k, int* lists, float* dists) {
             }
         }
     }
+}
+
+// orient_kruskal (MST.cpp:399-423) on host normals, in place.
+void orc_orient_kruskal(const int* knn, int64_t n, int k, int k_use, float* nx, float* ny, float* nz) {
+    orient_kruskal_impl(knn, n, k, k_use, nx, ny, nz);
 }
 
 }  // extern "C"

@@ -158,13 +158,81 @@ def save_digest(path, meta, inputs, outs, rows=256, seed=99):
     np.savez_compressed(path, **arrs)
 
 
+MST_LIB = os.path.join(ROOT, "oracle", "_ref", "libegtref_mst.so")
+
+
+def run_orient_kruskal(knn, nrm, k_use, xyz=None):
+    """The reference's CPU orient_kruskal (MST.cpp:399-423), unmodified, on
+    (n, k) lists and (3, n) normals; returns (normals, milliseconds)."""
+    lib = C.CDLL(MST_LIB)
+    f = lib.egtref_orient_kruskal
+    f.restype = C.c_double
+    f.argtypes = [C.c_void_p] * 7 + [C.c_int] * 3
+    knn = np.ascontiguousarray(knn, dtype=np.int32)
+    n, k = knn.shape
+    out = np.array(nrm, dtype=np.float32, order="C", copy=True)
+    pos = np.zeros((3, n), np.float32) if xyz is None else np.array(xyz, dtype=np.float32, order="C", copy=True)
+    ms = f(_p(knn), _p(out[0]), _p(out[1]), _p(out[2]), _p(pos[0]), _p(pos[1]), _p(pos[2]), n, k, int(k_use))
+    return out, ms
+
+
+def orient_cases():
+    """Inputs for the CPU-orienter fixtures: oracle kNN lists and unoriented
+    oracle PCA normals with seeded random signs.  Built with the CPU oracle
+    (oracle/pyoracle.py), which is test infrastructure like this script."""
+    from oracle import pyoracle
+    rng = np.random.default_rng(41)
+    cases = []
+    # a noisy sphere: one component, first 10 of 16 entries used
+    kn = pyoracle.knn(datagen.sphere_cloud(20000, 0.005, 42), 16)
+    nrm = pyoracle.normals(kn["pos"], kn["lists"])
+    nrm *= np.where(rng.random(nrm.shape[1]) < 0.5, -1.0, 1.0).astype(np.float32)
+    cases.append(("ref_orient_sphere.npz", "sphere_cloud(20000,0.005,42) k=16 oracle lists and PCA normals, random signs",
+                  kn["lists"], nrm, 10))
+    # two clouds that share no list edge, 20% of the entries blanked (-1, as the
+    # EGT filter leaves them), and five rows with no neighbours: several trees
+    a = pyoracle.knn(datagen.sphere_cloud(6000, 0.005, 43), 12)
+    b = pyoracle.knn(datagen.sphere_cloud(3000, 0.01, 44), 12)
+    lists = np.concatenate([a["lists"], np.where(b["lists"] >= 0, b["lists"] + 6000, -1),
+                            np.full((5, 12), -1, np.int32)]).astype(np.int32)
+    lists[rng.random(lists.shape) < 0.2] = -1
+    nrm = np.concatenate([pyoracle.normals(a["pos"], a["lists"]), pyoracle.normals(b["pos"], b["lists"]),
+                          np.tile(np.array([[0.0], [0.0], [1.0]], np.float32), (1, 5))], axis=1)
+    nrm *= np.where(rng.random(nrm.shape[1]) < 0.5, -1.0, 1.0).astype(np.float32)
+    cases.append(("ref_orient_forest.npz", "sphere_cloud(6000,0.005,43) + sphere_cloud(3000,0.01,44) k=12, "
+                  "20% of entries blanked, 5 empty rows; random signs", lists, nrm, 12))
+    # a lattice with every normal (0, 0, +-1): every weight is exactly 0, so
+    # the order is (u, v) alone and union-by-rank ties decide the roots
+    kn = pyoracle.knn(lattice_cloud(24), 8)
+    n = kn["lists"].shape[0]
+    nrm = np.zeros((3, n), np.float32)
+    nrm[2] = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+    cases.append(("ref_orient_ties.npz", "lattice_cloud(24) k=8 oracle lists, normals (0,0,+-1)", kn["lists"], nrm, 8))
+    return cases
+
+
+def make_orient(out_dir, timings):
+    for name, gen, lists, nrm, k_use in orient_cases():
+        o, ms = run_orient_kruskal(lists, nrm, k_use)
+        timings[name[:-4]] = ms
+        save_full(os.path.join(out_dir, name), dict(kind="orient_kruskal", gen=gen, k_use=int(k_use)),
+                  {"knn": lists, "nrm_in": nrm}, {"nrm_out": o})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
     ap.add_argument("--big", action="store_true", help="also run the 4M-point timing case")
     ap.add_argument("--only-query", action="store_true", help="only the query-vs-reference kNN fixtures")
+    ap.add_argument("--only-orient", action="store_true",
+                    help="only the CPU-orienter fixtures (MST.cpp; needs no GPU)")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
+    if a.only_orient:
+        t = {}
+        make_orient(a.out, t)
+        print(json.dumps(t))
+        return
     lib = load()
     timings = {}
 

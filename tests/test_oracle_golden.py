@@ -10,7 +10,7 @@ must sit within 1e-6 of the bounding-box diagonal of the FP64 oracle.
 import numpy as np
 import pytest
 
-from golden_util import FULL, MESH_FULL, bbox_diag, load, regen, sha
+from golden_util import FULL, MESH_FULL, ORIENT, bbox_diag, load, regen, sha
 
 
 @pytest.mark.parametrize("name", FULL)
@@ -104,3 +104,13 @@ def test_query_knn_bitexact(oracle, name):
     undefined = (status == 2) & (got[:, 0] < 0)
     assert (same | undefined).all()
     assert same[status != 2].all()
+
+
+@pytest.mark.parametrize("name", ORIENT)
+def test_orient_kruskal_bitexact(oracle, name):
+    """The CPU orienter orient_kruskal (MST.cpp:399-423): the restatement gives
+    the reference's normals bit for bit (one tree, a forest with empty rows,
+    all-equal weights)."""
+    d, m = load(name)
+    got = oracle.orient_kruskal(d["in_knn"], d["in_nrm_in"], m["k_use"])
+    assert np.array_equal(got.view(np.uint32), d["ref_nrm_out"].view(np.uint32))
