@@ -156,6 +156,23 @@ egt_status egt_knn_host(egt_handle* h, int k, int* knn_host, void* stream);
  * handle's configured threshold.  The handle's own lists are not changed. */
 egt_status egt_knn_query(egt_handle* h, const float* queries_host, int64_t nq, int k, int* knn_host,
                          int64_t* invalid, void* stream);
+/* orient_kruskal(knn, nx, ny, nz, x, y, z, N, k, k_use) (MST.cpp:399-423, with
+ * Graph::kruskalMST :297-376 and orientSpanningTree :262-279): the
+ * reference's CPU normal orienter, computed on the GPU with identical results.
+ * Host arrays, as in the reference: knn n*k ints (row i lists the neighbours of
+ * point i, entries < 0 are empty; only the first k_use of each row are read;
+ * an entry >= n is rejected with EGT_ERR_ARG), nx/ny/nz n floats each,
+ * oriented in place.  The edges are the distinct list pairs, weighted
+ * max(0, 1 - |n_u . n_v|) and ordered by (weight, u, v); each tree of the
+ * minimum spanning forest is walked from its union-find root, negating a
+ * normal whose dot product with its parent's is negative.  x, y, z are part
+ * of the reference's signature and are not read (they may be NULL).  The
+ * reference forms its edge key in 32-bit int arithmetic, which overflows
+ * above 46,340 points; this entry point uses 64-bit keys.  device: CUDA
+ * device ordinal; stream may be NULL. */
+egt_status egt_orient_kruskal(const int* knn, float* nx, float* ny, float* nz, const float* x, const float* y,
+                              const float* z, int n, int k, int k_use, int device, void* stream);
+
 /* Device pointers behind the KNNInterface getters. */
 egt_status egt_get_views(egt_handle* h, egt_views* views);
 /* Per-stage device timings of the last calls (filled when the stream is synced). */

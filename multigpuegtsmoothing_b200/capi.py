@@ -94,6 +94,7 @@ def lib() -> C.CDLL:
             "egt_knn": (i32, [vp, i32, vp]),
             "egt_knn_host": (i32, [vp, i32, vp, vp]),
             "egt_knn_query": (i32, [vp, vp, i64, i32, vp, C.POINTER(C.c_int64), vp]),
+            "egt_orient_kruskal": (i32, [vp, vp, vp, vp, vp, vp, vp, i32, i32, i32, i32, vp]),
             "egt_mesh_1ring": (i32, [vp, i32, vp]),
             "egt_smooth": (i32, [vp, i32, f32, f32, f32, vp]),
             "egt_filter": (i32, [vp, f32, vp]),
@@ -391,6 +392,26 @@ def getOutputPoints(provider: _Handle) -> Tuple[np.ndarray, np.ndarray, np.ndarr
     x, y, z = (np.empty(n, np.float32) for _ in range(3))
     _check(lib().egt_output(provider.handle, _ptr(x), _ptr(y), _ptr(z), provider.stream))
     return x, y, z
+
+
+def orient_kruskal(knn: np.ndarray, nx: np.ndarray, ny: np.ndarray, nz: np.ndarray, x=None, y=None, z=None,
+                   N: Optional[int] = None, k: Optional[int] = None, k_use: Optional[int] = None,
+                   device: int = 0) -> None:
+    """orient_kruskal(knn, nx, ny, nz, x, y, z, N, k, k_use) (MST.cpp:399-423):
+    the reference's CPU normal orienter, computed on the GPU.  knn: (N, k)
+    int32 (or flat N*k); nx, ny, nz: float32 arrays of N, oriented in place
+    (they must be contiguous float32).  x, y, z are not read."""
+    knn = np.ascontiguousarray(knn, dtype=np.int32)
+    for a in (nx, ny, nz):
+        if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous):
+            raise TypeError("orient_kruskal: nx, ny, nz must be contiguous float32 arrays (oriented in place)")
+    n = int(N) if N is not None else nx.shape[0]
+    kk = int(k) if k is not None else (knn.shape[1] if knn.ndim == 2 else knn.size // max(n, 1))
+    ku = int(k_use) if k_use is not None else kk
+    if knn.size < n * kk or min(nx.size, ny.size, nz.size) < n:
+        raise ValueError("orient_kruskal: arrays smaller than N*k / N")
+    _check(lib().egt_orient_kruskal(_ptr(knn), _ptr(nx), _ptr(ny), _ptr(nz), None, None, None, n, kk, ku,
+                                    int(device), None))
 
 
 PROPOSAL_PARAMS = 1872

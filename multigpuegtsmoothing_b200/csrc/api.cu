@@ -261,6 +261,43 @@ egt_status egt_knn_query(egt_handle* h, const float* queries_host, int64_t nq, i
     return run_knn_query(h, queries_host, nq, k, knn_host, invalid);
 }
 
+egt_status egt_orient_kruskal(const int* knn, float* nx, float* ny, float* nz, const float* x, const float* y,
+                              const float* z, int n, int k, int k_use, int device, void* stream) {
+    (void)x; (void)y; (void)z;  // in the reference's signature, not read by it either
+    if (n < 0 || k < 1 || k_use < 0 || k_use > k) {
+        set_error("egt_orient_kruskal: need n >= 0, k >= 1 and 0 <= k_use <= k");
+        return EGT_ERR_ARG;
+    }
+    if (n == 0 || k_use == 0) return EGT_OK;
+    if (!knn || !nx || !ny || !nz) { set_error("egt_orient_kruskal: null array"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(device));
+    cudaStream_t st = (cudaStream_t)stream;
+    int* d_knn = nullptr;
+    float* d_nrm = nullptr;
+    // whole rows: one contiguous copy (a strided copy of k_use columns from
+    // pageable memory goes row by row)
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&d_knn, sizeof(int) * (size_t)n * k, st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&d_nrm, sizeof(float) * 3 * (size_t)n, st));
+    egt_status s = EGT_OK;
+    cudaError_t e = cudaMemcpyAsync(d_knn, knn, sizeof(int) * (size_t)n * k, cudaMemcpyHostToDevice, st);
+    const float* src[3] = {nx, ny, nz};
+    for (int c = 0; c < 3 && e == cudaSuccess; c++)
+        e = cudaMemcpyAsync(d_nrm + (size_t)c * n, src[c], sizeof(float) * n, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { set_error(cuda_msg(e, "egt_orient_kruskal upload", __FILE__, __LINE__)); s = EGT_ERR_CUDA; }
+    if (s == EGT_OK) s = run_orient_kruskal(d_knn, d_nrm, n, k, k_use, st);
+    if (s == EGT_OK) {
+        float* dst[3] = {nx, ny, nz};
+        for (int c = 0; c < 3 && e == cudaSuccess; c++)
+            e = cudaMemcpyAsync(dst[c], d_nrm + (size_t)c * n, sizeof(float) * n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) { set_error(cuda_msg(e, "egt_orient_kruskal download", __FILE__, __LINE__)); s = EGT_ERR_CUDA; }
+    }
+    cudaFreeAsync(d_knn, st);
+    cudaFreeAsync(d_nrm, st);
+    cudaStreamSynchronize(st);
+    return s;
+}
+
 egt_status egt_knn_learned(egt_handle* h, int k, const egt_proposal* p, void* stream) {
     EGT_TRY(check_handle(h));
     if (!p) { set_error("egt_knn_learned: null proposal"); return EGT_ERR_ARG; }

@@ -226,6 +226,7 @@ egt_status csr_nnz(egt_handle* h, int64_t* out);
 egt_status run_taubin(egt_handle* h, int iters, float lambda, float mu);
 egt_status run_normals(egt_handle* h);
 egt_status run_orient(egt_handle* h);
+egt_status run_orient_kruskal(const int* knn, float* nrm, int n, int k, int k_use, cudaStream_t st);
 egt_status run_output(egt_handle* h, float* x, float* y, float* z);  // device outputs
 egt_status lists_original(egt_handle* h, int* out_dev);
 egt_status scatter_original(egt_handle* h, const float* soa_sorted, float* soa_orig);

@@ -208,6 +208,15 @@ def orient_cases():
     nrm = np.zeros((3, n), np.float32)
     nrm[2] = np.where(rng.random(n) < 0.5, -1.0, 1.0)
     cases.append(("ref_orient_ties.npz", "lattice_cloud(24) k=8 oracle lists, normals (0,0,+-1)", kn["lists"], nrm, 8))
+    # axis-aligned normals: dot products are exactly +-1 or exactly 0, so the
+    # trees cross edges whose dot product is zero, where the walk leaves the
+    # child's sign as it is
+    kn = pyoracle.knn(lattice_cloud(20, seed=45), 6)
+    n = kn["lists"].shape[0]
+    nrm = np.zeros((3, n), np.float32)
+    nrm[rng.integers(0, 3, n), np.arange(n)] = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+    cases.append(("ref_orient_zero.npz", "lattice_cloud(20,seed=45) k=6 oracle lists, random axis normals +-e_x/e_y/e_z",
+                  kn["lists"], nrm, 6))
     return cases
 
 

@@ -8,7 +8,7 @@ import numpy as np
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FULL = ["ref_sphere_small", "ref_lattice", "ref_dups"]
 MESH_FULL = ["ref_torus_small"]
-ORIENT = ["ref_orient_sphere", "ref_orient_forest", "ref_orient_ties"]
+ORIENT = ["ref_orient_sphere", "ref_orient_forest", "ref_orient_ties", "ref_orient_zero"]
 
 
 def load(name):
