@@ -1210,7 +1210,10 @@ int orc_orient(int n, int k, const int* lists, float* nrm, int* parent) {
 //     a depth-first walk with an explicit stack: pop u, then for each
 //     unprocessed neighbour v in adjacency order negate n_v when the float
 //     dot product of n_u and n_v is negative and push v; u is then processed.
-void orient_kruskal_impl(const int* knn, int64_t n, int k, int k_use, float* nx, float* ny, float* nz) {
+//   key32 != 0 forms the key as the reference does, N * u + v in 32-bit int
+//   arithmetic with two's-complement wrap-around (the reference's overflow),
+//   so that pairs whose keys collide are dropped as it drops them.
+void orient_kruskal_impl(const int* knn, int64_t n, int k, int k_use, float* nx, float* ny, float* nz, int key32) {
     struct Edge { double w; int u, v; };
     auto dotf = [&](int a, int b) {
         const float t = nx[a] * nx[b] + ny[a] * ny[b];
@@ -1224,7 +1227,9 @@ void orient_kruskal_impl(const int* knn, int64_t n, int k, int k_use, float* nx,
             const int m = knn[i * k + j];
             if (m < 0) continue;
             const int u = (int)std::min<int64_t>(i, m), v = (int)std::max<int64_t>(i, m);
-            if (!seen.insert((uint64_t)u * (uint64_t)n + (uint64_t)v).second) continue;
+            const uint64_t key = key32 ? (uint64_t)(int64_t)(int32_t)((uint32_t)n * (uint32_t)u + (uint32_t)v)
+                                       : (uint64_t)u * (uint64_t)n + (uint64_t)v;
+            if (!seen.insert(key).second) continue;
             const double d = (double)dotf((int)i, m);
             const double w = std::max(0.0, 1.0 - std::fabs(d));
             edges.push_back({w, u, v});
@@ -1307,9 +1312,10 @@ void orc_bruteforce(const float* pos, int n, int k, int* lists, float* dists) {
     }
 }
 
-// orient_kruskal (MST.cpp:399-423) on host normals, in place.
-void orc_orient_kruskal(const int* knn, int64_t n, int k, int k_use, float* nx, float* ny, float* nz) {
-    orient_kruskal_impl(knn, n, k, k_use, nx, ny, nz);
+// orient_kruskal (MST.cpp:399-423) on host normals, in place; key32 as in
+// orient_kruskal_impl.
+void orc_orient_kruskal(const int* knn, int64_t n, int k, int k_use, float* nx, float* ny, float* nz, int key32) {
+    orient_kruskal_impl(knn, n, k, k_use, nx, ny, nz, key32);
 }
 
 }  // extern "C"

@@ -43,7 +43,7 @@ def lib():
         L.orc_normals.argtypes = [vp, i32, i32, vp, i32, vp]
         L.orc_orient.restype = i32
         L.orc_orient.argtypes = [i32, i32, vp, vp, vp]
-        L.orc_orient_kruskal.argtypes = [vp, C.c_int64, i32, i32, vp, vp, vp]
+        L.orc_orient_kruskal.argtypes = [vp, C.c_int64, i32, i32, vp, vp, vp, i32]
         L.orc_output.argtypes = [vp, vp, vp, i32, vp]
         L.orc_bruteforce.argtypes = [vp, i32, i32, vp, vp]
         L.orc_knn_timed.argtypes = [vp, i32, i32, i32, vp, vp]
@@ -149,13 +149,15 @@ def orient(nrm: np.ndarray, lists: np.ndarray):
     return out, parent, nc
 
 
-def orient_kruskal(knn: np.ndarray, nrm: np.ndarray, k_use: int) -> np.ndarray:
+def orient_kruskal(knn: np.ndarray, nrm: np.ndarray, k_use: int, key32: bool = False) -> np.ndarray:
     """The reference's CPU orienter orient_kruskal (MST.cpp:399-423) on
-    (n, k) lists and (3, n) normals; returns the oriented (3, n) normals."""
+    (n, k) lists and (3, n) normals; returns the oriented (3, n) normals.
+    key32 reproduces the reference's 32-bit edge key, which wraps around
+    above 46,340 points (colliding pairs are then dropped)."""
     knn = np.ascontiguousarray(knn, dtype=np.int32)
     n, k = knn.shape
     out = np.array(nrm, dtype=np.float32, order="C", copy=True)
-    lib().orc_orient_kruskal(_p(knn), n, k, int(k_use), _p(out[0]), _p(out[1]), _p(out[2]))
+    lib().orc_orient_kruskal(_p(knn), n, k, int(k_use), _p(out[0]), _p(out[1]), _p(out[2]), int(key32))
     return out
 
 

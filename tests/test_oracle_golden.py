@@ -114,3 +114,29 @@ def test_orient_kruskal_bitexact(oracle, name):
     d, m = load(name)
     got = oracle.orient_kruskal(d["in_knn"], d["in_nrm_in"], m["k_use"])
     assert np.array_equal(got.view(np.uint32), d["ref_nrm_out"].view(np.uint32))
+
+
+def test_orient_kruskal_key_overflow_pinned(oracle):
+    """Above 46,340 points the reference's edge key N*u+v overflows its 32-bit
+    int (MST.cpp:404) and colliding pairs are dropped.  With the reference's
+    wrap-around key the restatement reproduces the unmodified MST.cpp bit for
+    bit on a 1M-point cloud, and the 64-bit key (the library's) differs from it
+    only there.  Runs where the reference was built (oracle/_ref)."""
+    import os
+    import sys
+    ref_lib = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                           "libegtref_mst.so")
+    if not os.path.exists(ref_lib):
+        pytest.skip("reference MST.cpp not built here")
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import run_orient_kruskal
+    from multigpuegtsmoothing_b200 import datagen
+    kn = oracle.knn(datagen.superquadrics(1_000_000, seed=3), 16)
+    nrm = oracle.normals(kn["pos"], kn["lists"])
+    rng = np.random.default_rng(51)
+    nrm *= np.where(rng.random(nrm.shape[1]) < 0.5, -1.0, 1.0).astype(np.float32)
+    ref, _ = run_orient_kruskal(kn["lists"], nrm, 10)
+    o32 = oracle.orient_kruskal(kn["lists"], nrm, 10, key32=True)
+    o64 = oracle.orient_kruskal(kn["lists"], nrm, 10)
+    assert np.array_equal(o32.view(np.uint32), ref.view(np.uint32))
+    assert (o64 != ref).any(0).sum() > 0  # the overflow matters at this size
