@@ -181,6 +181,26 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvidia-smi, 200 ms"}
 
 
+def fp32_rates(knn_evals, knn_ms, egt_tests, egt_ms, clk):
+    """kNN and EGT as FP32 operation rates from the counted evaluations: a
+    candidate distance is 3 subtractions, 1 multiply and 2 fused multiply-adds
+    (8 operations); an ellipsoid test is three 3-term affine transforms (6 each)
+    and the quadratic form (6).  Peak: 148 SMs x 128 FP32 lanes x 2 operations
+    per FMA at the SM clock sampled during the timed region (nominal, not
+    measured)."""
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+
+    def one(count, per, ms, what):
+        achieved = count * per / (ms * 1e-3) / 1e12 if ms > 0 else 0.0
+        return {"evaluations": int(count), "ops_per_evaluation": per, "what": what, "ms": ms,
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_kind": f"nominal FP32 at {mhz:.0f} MHz"}
+
+    return {"knn": one(knn_evals, 8, knn_ms, "candidate distances (k_knn_plain, timed step)"),
+            "egt": one(egt_tests, 24, egt_ms, "ellipsoid tests (k_egt)")}
+
+
 def dist_setup(init: bool = True):
     """Rank, world size and local rank from the torchrun environment; with
     init and more than one rank, joins the process group (NCCL with one GPU per
@@ -427,6 +447,7 @@ def run_b200(args, world, rank, local):
             capi.Normal_CUDA(g).GetNormals()
     t_egt, t_egt_kernel = tmf["egt_ms"], tmf["egt_kernel_ms"]
     nnz = tmf["csr_nnz"]
+    knn_evals, egt_tests = tm["knn_evaluations"], tmf["egt_tests"]
     egt.Taubin(ITERS)  # warm-up (graph capture path)
     torch.cuda.synchronize()
     ta, tb_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -488,6 +509,7 @@ def run_b200(args, world, rank, local):
                          "bytes_model": "n*(24+4k)"},
             "e2e": {"value": e2e_value, "unit": "Mqueries/s", "h2d_bytes_per_step": int(xyz.nbytes),
                     "d2h_bytes_per_step": int(n * K * 4)},
+            "fp32": fp32_rates(knn_evals, knn_ms, egt_tests, t_egt_kernel, clk),
             "gpu_launches": int(launches),
             "clocks": clk,
             "knn_stats": {"invalid_queries": tm["invalid_queries"], "levels_used": tm["levels_used"]},

@@ -88,6 +88,8 @@ typedef struct egt_timings {
     int64_t certified_queries; /* learned kNN: box results certified (the rest ran the plain search) */
     int64_t exact_reruns;    /* kNN queries whose kept distances tied and that were searched again
                                 with the reference's one-at-a-time insertion rule */
+    int64_t knn_evaluations; /* plain kNN: candidate distances evaluated (8 FP32 operations each) */
+    int64_t egt_tests;       /* EGT filter: ellipsoid tests evaluated (24 FP32 operations each) */
 } egt_timings;
 
 void egt_default_config(egt_config* cfg);

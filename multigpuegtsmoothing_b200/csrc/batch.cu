@@ -336,7 +336,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_egt_batch(const float4* __restr
     const int c = cloud[i];
     const int64_t o = off[c];
     const int k = kk[c];
-    const int cnt = egt_query<S>(p4 + o, p4[i], lists + loff[c] + (i - o) * k, k, alpha, lane);
+    unsigned tests = 0;  // not reported for batches
+    const int cnt = egt_query<S>(p4 + o, p4[i], lists + loff[c] + (i - o) * k, k, alpha, lane, tests);
     if (lane == 0) counts[i] = cnt;
 }
 

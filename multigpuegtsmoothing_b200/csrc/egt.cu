@@ -27,12 +27,35 @@ constexpr int kWarps = 8;
 
 template <int S>
 __global__ void __launch_bounds__(kWarps * 32) k_egt(const float4* __restrict__ p4, int* __restrict__ lists,
-                                                     int n, int k, float alpha, int* __restrict__ counts) {
+                                                     int n, int k, float alpha, int* __restrict__ counts,
+                                                     unsigned* __restrict__ tests_out) {
     const int lane = threadIdx.x & 31;
     const int q = blockIdx.x * kWarps + (threadIdx.x >> 5);
     if (q >= n) return;
-    const int cnt = egt_query<S>(p4, p4[q], lists + (size_t)q * k, k, alpha, lane);
-    if (lane == 0) counts[q] = cnt;
+    unsigned tests = 0;
+    const int cnt = egt_query<S>(p4, p4[q], lists + (size_t)q * k, k, alpha, lane, tests);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tests += __shfl_xor_sync(0xffffffffu, tests, o);
+    if (lane == 0) {
+        counts[q] = cnt;
+        tests_out[q] = tests;
+    }
+}
+
+// Sum of n counts into *out (one atomic per block).
+__global__ void k_sum_counts(const unsigned* __restrict__ in, int n, unsigned long long* __restrict__ out) {
+    __shared__ unsigned long long s_part[8];
+    unsigned long long acc = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc += in[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s_part[w];
+        if (t) atomicAdd(out, t);
+    }
 }
 
 // Packs the kept entries of each row, in list order, into CSR columns.
@@ -62,9 +85,9 @@ __global__ void k_count_valid(const int* __restrict__ lists, int n, int k, int* 
 }
 
 template <int S>
-egt_status launch_egt(egt_handle* h, float alpha, int* counts) {
+egt_status launch_egt(egt_handle* h, float alpha, int* counts, unsigned* tests) {
     const unsigned G = (unsigned)((h->n + kWarps - 1) / kWarps);
-    k_egt<S><<<G, kWarps * 32, 0, h->stream>>>(h->p4, h->lists, (int)h->n, h->k, alpha, counts);
+    k_egt<S><<<G, kWarps * 32, 0, h->stream>>>(h->p4, h->lists, (int)h->n, h->k, alpha, counts, tests);
     EGT_LAUNCH_CHECK();
     return EGT_OK;
 }
@@ -127,19 +150,27 @@ egt_status run_egt(egt_handle* h, float alpha) {
     cudaStream_t st = h->stream;
     const int64_t n = h->n;
     int* counts = nullptr;
+    unsigned* tests = nullptr;  // ellipsoid tests per query, summed for egt_get_timings
     EGT_CUDA_TRY(cudaMallocAsync((void**)&counts, sizeof(int) * (n + 1), st));
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&tests, sizeof(unsigned) * n, st));
     EGT_CUDA_TRY(cudaMemsetAsync(counts + n, 0, sizeof(int), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrEgtTests, 0, sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[4], st));
     const int k = h->k;
     egt_status s;
-    if (k <= 32) s = launch_egt<1>(h, alpha, counts);
-    else if (k <= 64) s = launch_egt<2>(h, alpha, counts);
-    else if (k <= 128) s = launch_egt<4>(h, alpha, counts);
-    else s = launch_egt<8>(h, alpha, counts);
+    if (k <= 32) s = launch_egt<1>(h, alpha, counts, tests);
+    else if (k <= 64) s = launch_egt<2>(h, alpha, counts, tests);
+    else if (k <= 128) s = launch_egt<4>(h, alpha, counts, tests);
+    else s = launch_egt<8>(h, alpha, counts, tests);
     EGT_CUDA_TRY(cudaEventRecord(h->ev[14], st));
     if (s == EGT_OK) s = build_csr(h, counts);
     EGT_CUDA_TRY(cudaEventRecord(h->ev[5], st));
+    if (s == EGT_OK) {
+        k_sum_counts<<<592, 256, 0, st>>>(tests, (int)n, h->d_counters + kCtrEgtTests);
+        EGT_LAUNCH_CHECK();
+    }
     cudaFreeAsync(counts, st);
+    cudaFreeAsync(tests, st);
     return s;
 }
 

@@ -1,7 +1,8 @@
 // Elliptic-Gabriel filter of one query's list (one warp), shared by the
 // single-cloud (egt.cu) and batched (batch.cu) kernels.  See egt.cu for the
 // reference correspondence.  Returns the number of kept entries (uniform);
-// dropped entries of `row` are set to -1.
+// dropped entries of `row` are set to -1.  tests counts the ellipsoid tests
+// this lane evaluated.
 #pragma once
 #include "egt_internal.cuh"
 
@@ -10,7 +11,7 @@ namespace {
 
 template <int S>
 __device__ __forceinline__ int egt_query(const float4* __restrict__ p4, float4 p, int* __restrict__ row, int k,
-                                         float alpha, int lane) {
+                                         float alpha, int lane, unsigned& tests) {
     int nb[S];
     float4 v[S];
     bool keep[S], test[S];
@@ -92,6 +93,7 @@ __device__ __forceinline__ int egt_query(const float4* __restrict__ p4, float4 p
         for (int s = 0; s < S; s++) {
             const int t = lane + 32 * s;
             if (test[s] && keep[s] && jp < t) {
+                ++tests;
                 const float lx = fs_affine(ax[s], ay[s], az[s], tx[s], ux, uy, uz);
                 const float ly = fs_affine(px[s], py[s], pz[s], ty[s], ux, uy, uz);
                 const float lz = fs_affine(qx[s], qy[s], qz[s], tz[s], ux, uy, uz);

@@ -109,6 +109,8 @@ constexpr int kCtrBoxTried = 40;  // learned kNN: queries that ran a box search
 constexpr int kCtrCertified = 41; // learned kNN: certified box results
 constexpr int kCtrExactRerun = 42;  // kNN queries re-searched with the exact insertion rule (ties)
 constexpr int kCtrWork = 43;        // work queue of the persistent kNN kernels (reset with 42)
+constexpr int kCtrEvals = 44;       // plain kNN: candidate distances evaluated (reset with 42)
+constexpr int kCtrEgtTests = 45;    // EGT filter: ellipsoid tests of the last filter run
 
 // One level of the cell hierarchy.  Cells are sorted by key
 // x + y*B + z*B^2; a row is the set of occupied cells sharing (y, z).

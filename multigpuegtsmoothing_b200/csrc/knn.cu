@@ -52,6 +52,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_plain(KnnArgs a
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const NormParams np = *a.np;
+    unsigned evals = 0;  // candidate distances this lane evaluated
     for (int q0 = claim(a, lane); q0 < a.n; q0 = claim(a, lane)) {
         const int q1 = min(q0 + a.chunk, a.n);
         for (int jq = q0; jq < q1; jq++) {
@@ -63,8 +64,12 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_plain(KnnArgs a
                                                       s_mp[w], rerun);
             write_query<S>(a, q, L, invalid, reached, lane);
             if (rerun && lane == 0) atomicAdd(&s_rerun, 1u);
+            evals += L.ev;
         }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
+    if (lane == 0 && evals) atomicAdd(&a.counters[kCtrEvals], (unsigned long long)evals);
     __syncthreads();
     if (threadIdx.x == 0 && s_rerun) atomicAdd(&a.counters[kCtrExactRerun], (unsigned long long)s_rerun);
 }
@@ -743,7 +748,7 @@ egt_status run_knn(egt_handle* h, int k) {
     KnnArgs a;
     EGT_TRY(knn_prepare(h, k, &a));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
-    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, 2 * sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, 3 * sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
     EGT_TRY(knn_launch(a, st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[3], st));
@@ -813,6 +818,7 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
     EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, t_sort, key, key2, idx, qmap, n, 0, bits, st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrEvals, 0, sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
     // streams: [0] = h->stream, [1] = a second search stream, [2] = copies
     cudaStream_t ss[3] = {st, nullptr, nullptr};
@@ -969,7 +975,7 @@ egt_status run_knn_learned(egt_handle* h, int k, const egt_proposal* p) {
     EGT_CUDA_TRY(cudaEventRecord(h->ev[15], st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrBoxTried, 0, 2 * sizeof(unsigned long long), st));
-    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, 2 * sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, 3 * sizeof(unsigned long long), st));
     KnnArgs a;
     a.p4 = h->p4;
     a.np = h->d_norm;

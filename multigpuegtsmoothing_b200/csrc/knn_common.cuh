@@ -26,6 +26,7 @@ struct WarpList {
     float kth;    // value of slot k-1 (uniform): 1e10 until the list is full
     int k;
     bool tie;     // an insertion met an equal distance already in the list
+    unsigned ev = 0;  // candidate distances this lane evaluated (not reset by init)
 
     __device__ __forceinline__ void init(int k_) {
 #pragma unroll

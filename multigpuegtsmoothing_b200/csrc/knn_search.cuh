@@ -240,6 +240,7 @@ __device__ __forceinline__ void stream_cells(WarpList<S>& L, bool& invalid, int 
             if (fresh) {
                 d = fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z);
                 ok = d <= thres;
+                ++L.ev;
             }
         }
         offer<kExact, S>(L, d, p, ok && d < L.kth, lane, s_md, s_mp);

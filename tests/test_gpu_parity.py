@@ -195,3 +195,24 @@ def test_chunked_knn_host_matches_search_then_copy(capi):
     # a second call on the same handle (buffers reused)
     assert np.array_equal(g2.knn_host(40), want)
     g2.close()
+
+
+def test_evaluation_counters(capi):
+    """The kNN candidate-distance and EGT ellipsoid-test counts behind the
+    bench's FP32 rates: every query evaluates at least k candidates, no query
+    tests more than k(k-1)/2 pairs, and the counts repeat exactly."""
+    xyz = datagen.sphere_cloud(20000, 0.005, 61)
+    k = 16
+    counts = []
+    for _ in range(2):
+        g = capi.GridStructure(xyz)
+        g.GRIDCUDAKNNSELF_COMPACT(k)
+        capi.EGT_CUDA(g).Filter(0.65)
+        t = g.timings()
+        counts.append((t["knn_evaluations"], t["egt_tests"]))
+        g.close()
+    ev, tests = counts[0]
+    n = xyz.shape[0]
+    assert ev >= n * k
+    assert 0 < tests <= n * k * (k - 1) // 2
+    assert counts[0] == counts[1]
