@@ -330,6 +330,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_egt_batch(const float4* __restr
                                                            const int64_t* __restrict__ loff,
                                                            const int* __restrict__ kk, int64_t N, float alpha,
                                                            int* __restrict__ counts) {
+    __shared__ float4 s_v[kWarps][32 * S];
     const int lane = threadIdx.x & 31;
     const int64_t i = blockIdx.x * (int64_t)kWarps + (threadIdx.x >> 5);
     if (i >= N) return;
@@ -337,7 +338,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_egt_batch(const float4* __restr
     const int64_t o = off[c];
     const int k = kk[c];
     unsigned tests = 0;  // not reported for batches
-    const int cnt = egt_query<S>(p4 + o, p4[i], lists + loff[c] + (i - o) * k, k, alpha, lane, tests);
+    const int cnt = egt_query<S>(p4 + o, p4[i], lists + loff[c] + (i - o) * k, k, alpha, lane, tests,
+                                 s_v[threadIdx.x >> 5]);
     if (lane == 0) counts[i] = cnt;
 }
 

@@ -29,11 +29,12 @@ template <int S>
 __global__ void __launch_bounds__(kWarps * 32) k_egt(const float4* __restrict__ p4, int* __restrict__ lists,
                                                      int n, int k, float alpha, int* __restrict__ counts,
                                                      unsigned* __restrict__ tests_out) {
+    __shared__ float4 s_v[kWarps][32 * S];
     const int lane = threadIdx.x & 31;
     const int q = blockIdx.x * kWarps + (threadIdx.x >> 5);
     if (q >= n) return;
     unsigned tests = 0;
-    const int cnt = egt_query<S>(p4, p4[q], lists + (size_t)q * k, k, alpha, lane, tests);
+    const int cnt = egt_query<S>(p4, p4[q], lists + (size_t)q * k, k, alpha, lane, tests, s_v[threadIdx.x >> 5]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) tests += __shfl_xor_sync(0xffffffffu, tests, o);
     if (lane == 0) {

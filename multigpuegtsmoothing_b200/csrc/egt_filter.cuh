@@ -11,7 +11,7 @@ namespace {
 
 template <int S>
 __device__ __forceinline__ int egt_query(const float4* __restrict__ p4, float4 p, int* __restrict__ row, int k,
-                                         float alpha, int lane, unsigned& tests) {
+                                         float alpha, int lane, unsigned& tests, float4* __restrict__ s_v) {
     int nb[S];
     float4 v[S];
     bool keep[S], test[S];
@@ -64,6 +64,14 @@ __device__ __forceinline__ int egt_query(const float4* __restrict__ p4, float4 p
     }
     const float aa = __fmul_rn(alpha, alpha);
     const float inv_aa = 1.0f / aa;
+    // the list's positions, read by the whole warp from shared memory (w: the
+    // neighbour index, -1 for an empty slot)
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        const int t = lane + 32 * s;
+        if (t < k) s_v[t] = make_float4(v[s].x, v[s].y, v[s].z, __int_as_float(nb[s]));
+    }
+    __syncwarp();
     // last slot index that still has something to test
     int hi = -1;
 #pragma unroll
@@ -71,40 +79,37 @@ __device__ __forceinline__ int egt_query(const float4* __restrict__ p4, float4 p
         if (test[s]) hi = lane + 32 * s;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    // Is slot s inside the ellipsoid of the closer neighbour u?  Estimated with
+    // a reciprocal (relative error < 1e-6 of the exact expression); the exact
+    // divisions decide only near the threshold.
+    auto inside = [&](int s, float4 u) {
+        const float lx = fs_affine(ax[s], ay[s], az[s], tx[s], u.x, u.y, u.z);
+        const float ly = fs_affine(px[s], py[s], pz[s], ty[s], u.x, u.y, u.z);
+        const float lz = fs_affine(qx[s], qy[s], qz[s], tz[s], u.x, u.y, u.z);
+        const float est = __fmaf_rn(lx, lx, __fmul_rn(__fmaf_rn(ly, ly, __fmul_rn(lz, lz)), inv_aa));
+        if (est < dd[s] * 0.99999f) return true;
+        if (est > dd[s] * 1.00001f) return false;
+        return fs_ellipsoid(lx, ly, lz, aa) < dd[s];
+    };
+    // The closer neighbours in list order, each read once by the whole warp.
+    // live[s]: slot s still has tests to run (it is tested and not rejected).
+    bool live[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) live[s] = test[s] && keep[s];
     for (int jp = 0; jp < hi; jp++) {
         if ((jp & 7) == 0) {  // stop once every slot with a pending test is decided
             bool pending = false;
 #pragma unroll
-            for (int s = 0; s < S; s++) pending |= test[s] && keep[s] && jp < lane + 32 * s;
+            for (int s = 0; s < S; s++) pending |= live[s] && jp < lane + 32 * s;
             if (!__any_sync(0xffffffffu, pending)) break;
         }
-        const int sl = jp & 31, ss = jp >> 5;
-        int bn = nb[0];
-        float4 bv = v[0];
-#pragma unroll
-        for (int s = 1; s < S; s++)
-            if (ss == s) { bn = nb[s]; bv = v[s]; }
-        bn = __shfl_sync(0xffffffffu, bn, sl);
-        if (bn < 0) continue;  // uniform
-        const float ux = __shfl_sync(0xffffffffu, bv.x, sl);
-        const float uy = __shfl_sync(0xffffffffu, bv.y, sl);
-        const float uz = __shfl_sync(0xffffffffu, bv.z, sl);
+        const float4 u = s_v[jp];
+        if (__float_as_int(u.w) < 0) continue;  // an empty slot (uniform)
 #pragma unroll
         for (int s = 0; s < S; s++) {
-            const int t = lane + 32 * s;
-            if (test[s] && keep[s] && jp < t) {
+            if (live[s] && jp < lane + 32 * s) {
                 ++tests;
-                const float lx = fs_affine(ax[s], ay[s], az[s], tx[s], ux, uy, uz);
-                const float ly = fs_affine(px[s], py[s], pz[s], ty[s], ux, uy, uz);
-                const float lz = fs_affine(qx[s], qy[s], qz[s], tz[s], ux, uy, uz);
-                // Estimate with a reciprocal (relative error < 1e-6 of the exact
-                // expression); the exact divisions decide only near the threshold.
-                const float est = __fmaf_rn(lx, lx, __fmul_rn(__fmaf_rn(ly, ly, __fmul_rn(lz, lz)), inv_aa));
-                bool inside;
-                if (est < dd[s] * 0.99999f) inside = true;
-                else if (est > dd[s] * 1.00001f) inside = false;
-                else inside = fs_ellipsoid(lx, ly, lz, aa) < dd[s];
-                if (inside) keep[s] = false;
+                if (inside(s, u)) { keep[s] = false; live[s] = false; }
             }
         }
     }
