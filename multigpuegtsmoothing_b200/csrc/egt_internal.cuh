@@ -180,7 +180,7 @@ struct egt_handle {
     // per 256-row tile: distinct neighbour indices (stored at the tile's first
     // CSR offset) and, per CSR entry, its index into that list
     int* t_uni = nullptr;        // [tiles * 1024] point index of each staged slot
-    uint16_t* t_loc = nullptr;   // [tiles * 5120] slot of each CSR entry, sliced by warp
+    uint32_t* t_loc = nullptr;   // [tiles * 1792] CSR entries' slots, three 10-bit slots per word, sliced by warp
     int* t_nu = nullptr;         // [tiles] staged slot count, -1 = tile not staged
     int* t_soff = nullptr;       // [tiles * 9] slice offsets into t_loc, then the table size
     int64_t t_tiles = 0;         // tiles the four tables above are sized for

@@ -107,12 +107,13 @@ __device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddep
 constexpr int kUCap = 1024;      // distinct neighbours staged per tile (16 KB; 99.8% of tiles fit)
 constexpr int kUPer = kUCap / kTile;  // staged positions per thread
 constexpr int kSlices = kTile / 32;   // one 32-row slice per warp
-constexpr int kSellCap = 5632;   // neighbour-slot entries per tile, slices padded to their longest row
-constexpr size_t kStageBytes = kUCap * sizeof(float4) + kSellCap * sizeof(uint16_t);
+constexpr int kSellWords = 1792; // 32-bit slot words per tile (three 10-bit slots each; every tile of the 4M workload fits)
+constexpr size_t kStageBytes = kUCap * sizeof(float4) + kSellWords * sizeof(uint32_t);
 constexpr int kStages = 2;       // tile buffers per block: one being computed, one being filled
 constexpr size_t kPipeSmem = kStages * kStageBytes;
 constexpr int kSoffWords = kSlices + 1;  // per tile: slice offsets and the tile's slot count
-static_assert(kSellCap % 8 == 0, "slot tiles are copied in 8-entry vectors");
+static_assert(kSellWords % 4 == 0, "slot tables are copied in 4-word vectors");
+static_assert(kUCap <= 1024, "slots are 10-bit");
 static_assert(kStageBytes % 16 == 0, "stage buffers stay 16-byte aligned");
 
 // 16-byte global -> shared copies that complete asynchronously (cp.async,
@@ -153,17 +154,17 @@ __device__ __forceinline__ TileRegs tile_regs(const int* __restrict__ off, const
     return r;
 }
 
-// Starts the copies of one tile into a stage buffer: the tile's 16-bit
-// neighbour slots (a fixed-stride, 16-byte aligned table) and its staged
-// positions (one 16-byte gather each).  Always commits one group.
+// Starts the copies of one tile into a stage buffer: the tile's packed
+// neighbour slots (a fixed-stride, 16-byte aligned table of 32-bit words) and
+// its staged positions (one 16-byte gather each).  Always commits one group.
 __device__ __forceinline__ void tile_fetch(const TileRegs& r, const float4* __restrict__ pin,
-                                           const uint16_t* __restrict__ t_loc, int tile, unsigned char* stage) {
+                                           const uint32_t* __restrict__ t_loc, int tile, unsigned char* stage) {
     if (r.nu >= 0) {
         float4* s_pos = reinterpret_cast<float4*>(stage);
-        uint16_t* s_loc = reinterpret_cast<uint16_t*>(stage + kUCap * sizeof(float4));
-        const uint16_t* src = t_loc + (size_t)tile * kSellCap;
-        const int nvec = (r.ssize + 7) >> 3;
-        for (int v = (int)threadIdx.x; v < nvec; v += kTile) cp_async16(s_loc + 8 * v, src + 8 * v);
+        uint32_t* s_loc = reinterpret_cast<uint32_t*>(stage + kUCap * sizeof(float4));
+        const uint32_t* src = t_loc + (size_t)tile * kSellWords;
+        const int nvec = (r.ssize + 3) >> 2;
+        for (int v = (int)threadIdx.x; v < nvec; v += kTile) cp_async16(s_loc + 4 * v, src + 4 * v);
 #pragma unroll
         for (int u = 0; u < kUPer; u++) {
             const int j = (int)threadIdx.x + u * kTile;
@@ -183,14 +184,16 @@ __device__ __forceinline__ void tile_fetch(const TileRegs& r, const float4* __re
 // memory once per tile; each row reads its neighbours from shared memory in
 // list order.  Tiles that do not fit (t_nu < 0) gather from global memory.
 //
-// The slots are sliced in groups of four: warp w's 32 rows (ordered by
-// decreasing neighbour count, see morton_prepare) store entries 4g..4g+3 of
-// lane l at soff[w] + 128 g + 4 l, so each step of a warp (four neighbours per
-// lane) reads 256 contiguous bytes of slots.
+// The slots are 10 bits, three to a 32-bit word, sliced by warp: warp w's 32
+// rows (ordered by decreasing neighbour count, see morton_prepare) store
+// entries 3g..3g+2 of lane l in word soff[w] + 32 g + l, so each step of a
+// warp (three neighbours per lane) reads 128 contiguous bytes of slots.  The
+// staged tables are what most of the kernel's DRAM traffic is made of; packed
+// this way they take 1.3 bytes per entry.
 __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restrict__ pin, float4* __restrict__ pout,
                                                         const int* __restrict__ off, const int* __restrict__ col,
                                                         const int* __restrict__ t_uni,
-                                                        const uint16_t* __restrict__ t_loc,
+                                                        const uint32_t* __restrict__ t_loc,
                                                         const int* __restrict__ t_nu, const int* __restrict__ t_soff,
                                                         int n, int tiles, float scale) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -229,28 +232,26 @@ __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restr
                     accumulate(p.x, p.y, p.z, __ldg(pin + __ldg(col + e)), cx, cy, cz, sum);
             } else {
                 const float4* s_pos = reinterpret_cast<const float4*>(stage);
-                const uint2* ls =
-                    reinterpret_cast<const uint2*>(stage + kUCap * sizeof(float4) + 2 * cur.soff) + lane;
+                const uint32_t* ls =
+                    reinterpret_cast<const uint32_t*>(stage + kUCap * sizeof(float4)) + cur.soff + lane;
                 const int len = cur.e1 - cur.e0;
-                // four neighbours per step; the next step's slot word is loaded
+                // three neighbours per step; the next step's slot word is loaded
                 // before this step's positions are read, off the critical path
                 int e = 0;
-                uint2 v = len > 0 ? ls[0] : make_uint2(0u, 0u);
+                uint32_t v = len > 0 ? ls[0] : 0u;
 #pragma unroll 1
-                for (; e + 4 <= len; e += 4) {
-                    const uint2 vn = e + 4 < len ? ls[8 * (e + 4)] : v;
-                    const float4 q0 = s_pos[v.x & 0xffff], q1 = s_pos[v.x >> 16];
-                    const float4 q2 = s_pos[v.y & 0xffff], q3 = s_pos[v.y >> 16];
+                for (; e + 3 <= len; e += 3) {
+                    ls += 32;
+                    const uint32_t vn = e + 3 < len ? *ls : v;
+                    const float4 q0 = s_pos[v & 1023u], q1 = s_pos[(v >> 10) & 1023u], q2 = s_pos[v >> 20];
                     accumulate(p.x, p.y, p.z, q0, cx, cy, cz, sum);
                     accumulate(p.x, p.y, p.z, q1, cx, cy, cz, sum);
                     accumulate(p.x, p.y, p.z, q2, cx, cy, cz, sum);
-                    accumulate(p.x, p.y, p.z, q3, cx, cy, cz, sum);
                     v = vn;
                 }
                 if (e < len) {
-                    accumulate(p.x, p.y, p.z, s_pos[v.x & 0xffff], cx, cy, cz, sum);
-                    if (e + 1 < len) accumulate(p.x, p.y, p.z, s_pos[v.x >> 16], cx, cy, cz, sum);
-                    if (e + 2 < len) accumulate(p.x, p.y, p.z, s_pos[v.y & 0xffff], cx, cy, cz, sum);
+                    accumulate(p.x, p.y, p.z, s_pos[v & 1023u], cx, cy, cz, sum);
+                    if (e + 1 < len) accumulate(p.x, p.y, p.z, s_pos[(v >> 10) & 1023u], cx, cy, cz, sum);
                 }
             }
             pout[i] = finish(p, cx, cy, cz, sum, scale);
@@ -268,18 +269,18 @@ __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restr
 // Builds the tables of one tile (one block per tile): a block radix sort of
 // the tile's column indices and a unique pass give the distinct neighbours
 // (t_uni, at a fixed stride of kUCap per tile) and each CSR entry's index
-// into them, a 16-bit slot; the slots are stored sliced by warp (warp w's 32
-// rows padded to its longest row rounded up to 4, entry 4g + r of lane l at
-// soff[w] + 128 g + 4 l + r, t_soff = soff[0..8] with soff[8] the table
-// size).  t_nu = the distinct
+// into them, a 10-bit slot; the slots are stored three to a 32-bit word,
+// sliced by warp (warp w's 32 rows padded to its longest row rounded up to 3,
+// entry 3g + j of lane l in bits 10j..10j+9 of word soff[w] + 32 g + l;
+// t_soff = soff[0..8] in words, soff[8] the table size).  t_nu = the distinct
 // count, or -1 when the tile does not fit (too many entries, distinct
-// neighbours or padded slots): its rows then gather from global memory.
+// neighbours or slot words): its rows then gather from global memory.
 constexpr int kBuildThreads = 512;
 constexpr int kBuildItems = kTileCap / kBuildThreads;
 
 __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restrict__ off, const int* __restrict__ col,
                                                               int n, int* __restrict__ t_uni,
-                                                              uint16_t* __restrict__ t_loc, int* __restrict__ t_nu,
+                                                              uint32_t* __restrict__ t_loc, int* __restrict__ t_nu,
                                                               int* __restrict__ t_soff) {
     using Sort = cub::BlockRadixSort<int, kBuildThreads, kBuildItems>;
     using Scan = cub::BlockScan<int, kBuildThreads>;
@@ -353,11 +354,11 @@ __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restr
         for (int w = 0; w < kSlices; w++) {
             int wmax = 0;
             for (int l = 0; l < 32; l++) wmax = max(wmax, s_len[32 * w + l]);
-            s_soff[w + 1] = s_soff[w] + 32 * ((wmax + 3) & ~3);
+            s_soff[w + 1] = s_soff[w] + 32 * ((wmax + 2) / 3);
         }
     }
     __syncthreads();
-    if (s_soff[kSlices] > kSellCap) {
+    if (s_soff[kSlices] > kSellWords) {
         if (threadIdx.x == 0) t_nu[tile] = -1;
         return;
     }
@@ -366,8 +367,13 @@ __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restr
     for (int x = threadIdx.x; x < ssize; x += kBuildThreads) {
         int w = 0;
         while (x >= s_soff[w + 1]) w++;
-        const int rel = x - s_soff[w], e = 4 * (rel >> 7) + (rel & 3), r = 32 * w + ((rel >> 2) & 31);
-        t_loc[(size_t)tile * kSellCap + x] = e < s_len[r] ? s_u[s_start[r] + e] : (uint16_t)0;
+        const int rel = x - s_soff[w], g = rel >> 5, r = 32 * w + (rel & 31);
+        uint32_t word = 0;
+        for (int j = 0; j < 3; j++) {
+            const int e = 3 * g + j;
+            if (e < s_len[r]) word |= (uint32_t)s_u[s_start[r] + e] << (10 * j);
+        }
+        t_loc[(size_t)tile * kSellWords + x] = word;
     }
     if (threadIdx.x < kSoffWords) t_soff[(size_t)tile * kSoffWords + threadIdx.x] = s_soff[threadIdx.x];
     if (threadIdx.x == 0) t_nu[tile] = nu;
@@ -487,7 +493,7 @@ static egt_status staged_launch(egt_handle* h, const float4* pin, float4* pout, 
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     EGT_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_taubin_tiles, pin, pout, (const int*)h->m_off, (const int*)h->m_col,
-                                    (const int*)h->t_uni, (const uint16_t*)h->t_loc, (const int*)h->t_nu,
+                                    (const int*)h->t_uni, (const uint32_t*)h->t_loc, (const int*)h->t_nu,
                                     (const int*)h->t_soff, n, tiles, scale));
     EGT_LAUNCH_CHECK();
     return EGT_OK;
@@ -570,7 +576,7 @@ static egt_status morton_prepare(egt_handle* h) {
             h->t_uni = nullptr; h->t_loc = nullptr; h->t_nu = nullptr; h->t_soff = nullptr;
             h->t_tiles = 0;
             EGT_CUDA_TRY(dev_alloc(h, &h->t_uni, sizeof(int) * kUCap * tiles));
-            EGT_CUDA_TRY(dev_alloc(h, &h->t_loc, sizeof(uint16_t) * kSellCap * tiles));
+            EGT_CUDA_TRY(dev_alloc(h, &h->t_loc, sizeof(uint32_t) * kSellWords * tiles));
             EGT_CUDA_TRY(dev_alloc(h, &h->t_nu, sizeof(int) * tiles));
             EGT_CUDA_TRY(dev_alloc(h, &h->t_soff, sizeof(int) * kSoffWords * tiles));
             h->t_tiles = tiles;
