@@ -757,11 +757,20 @@ egt_status run_knn(egt_handle* h, int k) {
 
 namespace {
 // Sort key of sorted slot s for the chunked search: the chunk of its original row.
-__global__ void k_chunk_keys(const int* __restrict__ perm, int n, int rows, uint32_t* __restrict__ key,
+constexpr int kMaxHostChunks = 16;
+struct ChunkBounds {
+    int end[kMaxHostChunks];  // chunk c holds the original rows [end[c-1], end[c])
+    int count;
+};
+
+__global__ void k_chunk_keys(const int* __restrict__ perm, int n, ChunkBounds cb, uint32_t* __restrict__ key,
                              int* __restrict__ idx) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    key[s] = (uint32_t)(perm[s] / rows);
+    const int r = perm[s];
+    uint32_t c = 0;
+    while ((int)c + 1 < cb.count && r >= cb.end[c]) c++;
+    key[s] = c;
     idx[s] = s;
 }
 
@@ -784,18 +793,32 @@ __global__ void k_rows_original(const int* __restrict__ lists, const int* __rest
 // its spatial locality).  Chunks alternate between two streams, so one
 // chunk's tail overlaps the next chunk's start, and each finished chunk's
 // rows -- a contiguous block of the original-order output -- are copied to
-// the host on a third stream while later chunks are searched.  The handle's
-// sorted-space lists are filled as egt_knn fills them.
-#ifndef EGT_KNN_HOST_CHUNKS
-#define EGT_KNN_HOST_CHUNKS 8
-#endif
+// the host on a third stream while later chunks are searched.  The chunks
+// shrink towards the end (20 % of the rows first, 1.5 % last): the copy of
+// the last chunk is the part that nothing overlaps, and each copy still
+// finishes before the next chunk's search (copying runs at about 0.6 of the
+// search rate).  The handle's sorted-space lists are filled as egt_knn fills
+// them.
 egt_status run_knn_host(egt_handle* h, int k, int* host) {
     cudaStream_t st = h->stream;
     KnnArgs a;
     EGT_TRY(knn_prepare(h, k, &a));
     const int n = (int)h->n;
-    const int chunks = std::max(1, std::min(EGT_KNN_HOST_CHUNKS, n / 131072));
-    const int rows = (n + chunks - 1) / chunks;
+    ChunkBounds cb{};
+    {
+        static const double kShare[] = {0.2, 0.2, 0.2, 0.15, 0.1, 0.07, 0.04, 0.025, 0.015};
+        const int parts = n >= 262144 ? (int)(sizeof(kShare) / sizeof(kShare[0])) : 1;
+        double acc = 0.0;
+        cb.count = 0;
+        for (int c = 0; c < parts; c++) {
+            acc += kShare[c];
+            const int e = c == parts - 1 ? n : std::min(n, (int)(acc * n));
+            if (cb.count > 0 && e <= cb.end[cb.count - 1]) continue;
+            cb.end[cb.count++] = e;
+        }
+        if (parts == 1) cb.end[0] = n;
+    }
+    const int chunks = cb.count;
     int bits = 1;
     while ((1 << bits) < chunks) bits++;
     uint32_t *key = nullptr, *key2 = nullptr;
@@ -809,7 +832,7 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
     EGT_CUDA_TRY(cudaMallocAsync((void**)&work, sizeof(unsigned long long) * chunks, st));
     EGT_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long) * chunks, st));
     const unsigned T = 256;
-    k_chunk_keys<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(h->perm, n, rows, key, idx);
+    k_chunk_keys<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(h->perm, n, cb, key, idx);
     EGT_LAUNCH_CHECK();
     size_t t_sort = 0;
     EGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, t_sort, key, key2, idx, qmap, n, 0, bits, st));
@@ -835,8 +858,8 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
     if (s == EGT_OK) fail(cudaEventRecord(ev[2 * chunks], st), "cudaEventRecord");
     if (s == EGT_OK) fail(cudaStreamWaitEvent(ss[1], ev[2 * chunks], 0), "cudaStreamWaitEvent");
     for (int c = 0; c < chunks && s == EGT_OK; c++) {
-        const int r0 = c * rows, m = std::min(rows, n - r0);
-        if (m <= 0) break;
+        const int r0 = c == 0 ? 0 : cb.end[c - 1], m = cb.end[c] - r0;
+        if (m <= 0) continue;
         cudaStream_t cs = ss[c & 1];
         // the chunk's sorted slots sit at qmap[r0, r0 + m): every chunk holds exactly its row count
         KnnArgs ac = a;

@@ -180,7 +180,7 @@ def test_superquadrics_4m_digest(capi):
 def test_chunked_knn_host_matches_search_then_copy(capi):
     """egt_knn_host (search in chunks of original rows, host copies overlapped)
     returns what egt_knn + egt_get_knn_host return, and leaves the same
-    sorted-space lists on the handle; 600K points run as 4 chunks."""
+    sorted-space lists on the handle; 600K points run as 9 chunks of decreasing size."""
     xyz = datagen.superquadrics(600_000, seed=7)
     g = cloud(capi, xyz, 40)
     want = g.GetKNNIndexes()
