@@ -1,25 +1,34 @@
-// Elliptic-Gabriel filter of one query's list (one warp), shared by the
-// single-cloud (egt.cu) and batched (batch.cu) kernels.  See egt.cu for the
-// reference correspondence.  Returns the number of kept entries (uniform);
-// dropped entries of `row` are set to -1.  tests counts the ellipsoid tests
-// this lane evaluated.
+// Elliptic-Gabriel filter of one query's list, shared by the single-cloud
+// (egt.cu) and batched (batch.cu) kernels.  See egt.cu for the reference
+// correspondence.  A query takes a group of G lanes (G = 32: one query per
+// warp; G = 16: two, which keeps more lanes busy when k does not fill whole
+// 32-slot rounds); slot t of the list sits on lane t % G of the group, round
+// t / G.  Every lane of the warp calls it (an `active` false group filters
+// nothing and writes nothing).  Returns the number of kept entries (uniform
+// over the group); dropped entries of `row` are set to -1.  tests counts the
+// ellipsoid tests this lane evaluated; s_v is the group's own staging
+// buffer.
 #pragma once
 #include "egt_internal.cuh"
 
 namespace egt {
 namespace {
 
-template <int S>
+template <int S, int G = 32>
 __device__ __forceinline__ int egt_query(const float4* __restrict__ p4, float4 p, int* __restrict__ row, int k,
-                                         float alpha, int lane, unsigned& tests, float4* __restrict__ s_v) {
+                                         float alpha, int lane, unsigned& tests, float4* __restrict__ s_v,
+                                         bool active = true) {
+    static_assert(G == 16 || G == 32, "groups of 16 or 32 lanes");
+    const unsigned gmask = G == 32 ? 0xffffffffu : (0xffffu << (lane & 16));
+    lane &= G - 1;  // from here on: the lane within the group
     int nb[S];
     float4 v[S];
     bool keep[S], test[S];
     float ax[S], ay[S], az[S], px[S], py[S], pz[S], qx[S], qy[S], qz[S], tx[S], ty[S], tz[S], dd[S];
 #pragma unroll
     for (int s = 0; s < S; s++) {
-        const int t = lane + 32 * s;
-        nb[s] = t < k ? row[t] : -1;
+        const int t = lane + G * s;
+        nb[s] = active && t < k ? row[t] : -1;
         v[s] = nb[s] >= 0 ? p4[nb[s]] : make_float4(0.f, 0.f, 0.f, 0.f);
         keep[s] = nb[s] != -1;
         test[s] = false;
@@ -68,15 +77,16 @@ __device__ __forceinline__ int egt_query(const float4* __restrict__ p4, float4 p
     // neighbour index, -1 for an empty slot)
 #pragma unroll
     for (int s = 0; s < S; s++) {
-        const int t = lane + 32 * s;
+        const int t = lane + G * s;
         if (t < k) s_v[t] = make_float4(v[s].x, v[s].y, v[s].z, __int_as_float(nb[s]));
     }
     __syncwarp();
-    // last slot index that still has something to test
+    // last slot index that still has something to test, over the whole warp
+    // (a group past its own last slot tests nothing)
     int hi = -1;
 #pragma unroll
     for (int s = 0; s < S; s++)
-        if (test[s]) hi = lane + 32 * s;
+        if (test[s]) hi = lane + G * s;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
     // Is slot s inside the ellipsoid of the closer neighbour u?  Estimated with
@@ -100,14 +110,14 @@ __device__ __forceinline__ int egt_query(const float4* __restrict__ p4, float4 p
         if ((jp & 7) == 0) {  // stop once every slot with a pending test is decided
             bool pending = false;
 #pragma unroll
-            for (int s = 0; s < S; s++) pending |= live[s] && jp < lane + 32 * s;
+            for (int s = 0; s < S; s++) pending |= live[s] && jp < lane + G * s;
             if (!__any_sync(0xffffffffu, pending)) break;
         }
-        const float4 u = s_v[jp];
-        if (__float_as_int(u.w) < 0) continue;  // an empty slot (uniform)
+        const float4 u = s_v[jp];  // jp < hi < k
+        const bool filled = __float_as_int(u.w) >= 0;  // not an empty slot (uniform over the group)
 #pragma unroll
         for (int s = 0; s < S; s++) {
-            if (live[s] && jp < lane + 32 * s) {
+            if (filled && live[s] && jp < lane + G * s) {
                 ++tests;
                 if (inside(s, u)) { keep[s] = false; live[s] = false; }
             }
@@ -116,9 +126,9 @@ __device__ __forceinline__ int egt_query(const float4* __restrict__ p4, float4 p
     int cnt = 0;
 #pragma unroll
     for (int s = 0; s < S; s++) {
-        const int t = lane + 32 * s;
-        if (t < k && nb[s] != -1 && !keep[s]) row[t] = -1;
-        cnt += __popc(__ballot_sync(0xffffffffu, keep[s]));
+        const int t = lane + G * s;
+        if (active && t < k && nb[s] != -1 && !keep[s]) row[t] = -1;
+        cnt += __popc(__ballot_sync(0xffffffffu, keep[s]) & gmask);
     }
     return cnt;
 }
