@@ -206,6 +206,14 @@ inline void getOutputPoints(float* x, float* y, float* z, KNNInterface* p) {
     check(egt_output(q.handle(), x, y, z, q.stream()), "getOutputPoints");
 }
 
+// orient_kruskal(knn, nx, ny, nz, x, y, z, N, k, k_use) (MST.h:11-12,
+// MST.cpp:399-423): the reference's CPU orienter, same signature, computed on
+// GPU 0 with the same oriented normals (see egt_orient_kruskal).
+inline void orient_kruskal(int* knn, float* nx, float* ny, float* nz, float* x, float* y, float* z, int N, int k,
+                           int k_use) {
+    check(egt_orient_kruskal(knn, nx, ny, nz, x, y, z, N, k, k_use, 0, nullptr), "orient_kruskal");
+}
+
 }  // namespace egtb200
 
 #endif  // EGT_KNN_INTERFACE_HPP
