@@ -68,3 +68,51 @@ def test_orient_kruskal_rejects_bad_input(capi):
         capi.orient_kruskal(knn, nx, ny, nz, k_use=3)  # k_use > k
     # k_use = 1 never reads the bad entry
     capi.orient_kruskal(knn, nx, ny, nz, k_use=1)
+
+
+CPP_CALLER = r"""
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#include "egt_knn_interface.hpp"
+int main(int argc, char** argv) {
+    const int n = std::atoi(argv[1]), k = std::atoi(argv[2]), k_use = std::atoi(argv[3]);
+    std::vector<int> knn((size_t)n * k);
+    std::vector<float> nrm((size_t)3 * n);
+    FILE* f = std::fopen(argv[4], "rb");
+    if (!f || std::fread(knn.data(), 4, knn.size(), f) != knn.size() ||
+        std::fread(nrm.data(), 4, nrm.size(), f) != nrm.size()) return 2;
+    std::fclose(f);
+    egtb200::orient_kruskal(knn.data(), nrm.data(), nrm.data() + n, nrm.data() + 2 * n, nullptr, nullptr,
+                            nullptr, n, k, k_use);
+    f = std::fopen(argv[5], "wb");
+    if (!f || std::fwrite(nrm.data(), 4, nrm.size(), f) != nrm.size()) return 3;
+    std::fclose(f);
+    return 0;
+}
+"""
+
+
+def test_cpp_adapter_orient_kruskal(tmp_path):
+    """A C++ caller of the reference's free function, switched to the adapter
+    header (include/egt_knn_interface.hpp), gets the reference's normals."""
+    import os
+    import shutil
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else shutil.which("g++")
+    lib = os.path.join(root, "multigpuegtsmoothing_b200", "lib")
+    src = tmp_path / "caller.cpp"
+    src.write_text(CPP_CALLER)
+    exe = tmp_path / "caller"
+    subprocess.run([cxx, "-std=c++17", "-O1", "-I", os.path.join(root, "include"), str(src), "-L", lib,
+                    "-legt_b200", f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True)
+    d, m = load("ref_orient_forest")
+    knn = np.ascontiguousarray(d["in_knn"], dtype=np.int32)
+    nrm = np.ascontiguousarray(d["in_nrm_in"], dtype=np.float32)
+    n, k = knn.shape
+    (tmp_path / "in.bin").write_bytes(knn.tobytes() + nrm.tobytes())
+    subprocess.run([str(exe), str(n), str(k), str(m["k_use"]), str(tmp_path / "in.bin"), str(tmp_path / "out.bin")],
+                   check=True)
+    got = np.frombuffer((tmp_path / "out.bin").read_bytes(), dtype=np.uint32).reshape(3, n)
+    assert np.array_equal(got, d["ref_nrm_out"].view(np.uint32))
