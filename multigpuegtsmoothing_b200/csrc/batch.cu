@@ -323,24 +323,28 @@ __global__ void __launch_bounds__(kWarps * 32) k_knn_batch(const KnnArgs* __rest
     }
 }
 
-template <int S>
-__global__ void __launch_bounds__(kWarps * 32) k_egt_batch(const float4* __restrict__ p4, int* __restrict__ lists,
-                                                           const uint16_t* __restrict__ cloud,
-                                                           const int64_t* __restrict__ off,
-                                                           const int64_t* __restrict__ loff,
-                                                           const int* __restrict__ kk, int64_t N, float alpha,
-                                                           int* __restrict__ counts) {
-    __shared__ float4 s_v[kWarps][32 * S];
+// One query per group of G lanes (32 / G queries per warp, possibly of
+// different clouds: each group filters with its own cloud's k).
+template <int S, int G>
+__global__ void __launch_bounds__(kWarps * 32, S <= 3 ? 4 : 1) k_egt_batch(
+    const float4* __restrict__ p4, int* __restrict__ lists, const uint16_t* __restrict__ cloud,
+    const int64_t* __restrict__ off, const int64_t* __restrict__ loff, const int* __restrict__ kk, int64_t N,
+    float alpha, int* __restrict__ counts) {
+    constexpr int kPer = 32 / G;
+    __shared__ float4 s_v[kWarps * kPer][G * S];
     const int lane = threadIdx.x & 31;
-    const int64_t i = blockIdx.x * (int64_t)kWarps + (threadIdx.x >> 5);
-    if (i >= N) return;
-    const int c = cloud[i];
+    const int64_t i0 = (blockIdx.x * (int64_t)kWarps + (threadIdx.x >> 5)) * kPer;
+    if (i0 >= N) return;  // whole warps only
+    const int64_t i = i0 + lane / G;
+    const bool active = i < N;
+    const int c = active ? cloud[i] : 0;
     const int64_t o = off[c];
     const int k = kk[c];
     unsigned tests = 0;  // not reported for batches
-    const int cnt = egt_query<S>(p4 + o, p4[i], lists + loff[c] + (i - o) * k, k, alpha, lane, tests,
-                                 s_v[threadIdx.x >> 5]);
-    if (lane == 0) counts[i] = cnt;
+    const int cnt = egt_query<S, G>(p4 + o, active ? p4[i] : make_float4(0.f, 0.f, 0.f, 0.f),
+                                    lists + loff[c] + (active ? i - o : 0) * k, k, alpha, lane, tests,
+                                    s_v[(threadIdx.x >> 5) * kPer + lane / G], active);
+    if (active && (lane & (G - 1)) == 0) counts[i] = cnt;
 }
 
 __global__ void k_count_batch(const int* __restrict__ lists, const uint16_t* __restrict__ cloud,
@@ -408,10 +412,10 @@ __global__ void k_lists_cloud(const int* __restrict__ lists, const int* __restri
 
 unsigned blocks(int64_t n, int per = kB) { return (unsigned)((n + per - 1) / per); }
 
-template <int S>
+template <int S, int G>
 egt_status launch_egt_batch(egt_batch* b, float alpha, int* counts, cudaStream_t st) {
-    k_egt_batch<S><<<blocks(b->N, kWarps), kWarps * 32, 0, st>>>(b->h->p4, b->h->lists, b->d_cloud, b->d_off,
-                                                                 b->d_loff, b->d_k, b->N, alpha, counts);
+    k_egt_batch<S, G><<<blocks(b->N, kWarps * (32 / G)), kWarps * 32, 0, st>>>(
+        b->h->p4, b->h->lists, b->d_cloud, b->d_off, b->d_loff, b->d_k, b->N, alpha, counts);
     EGT_LAUNCH_CHECK();
     return EGT_OK;
 }
@@ -523,10 +527,13 @@ egt_status filter_batch(egt_batch* b, float alpha) {
     EGT_CUDA_TRY(cudaEventRecord(b->h->ev[4], st));
     const int kk = b->kmax;
     egt_status s;
-    if (kk <= 32) s = launch_egt_batch<1>(b, alpha, counts, st);
-    else if (kk <= 64) s = launch_egt_batch<2>(b, alpha, counts, st);
-    else if (kk <= 128) s = launch_egt_batch<4>(b, alpha, counts, st);
-    else s = launch_egt_batch<8>(b, alpha, counts, st);
+    // lanes per query as in the single-cloud filter, from the largest k of the batch
+    if (kk <= 16) s = launch_egt_batch<1, 16>(b, alpha, counts, st);
+    else if (kk <= 32) s = launch_egt_batch<1, 32>(b, alpha, counts, st);
+    else if (kk <= 48) s = launch_egt_batch<3, 16>(b, alpha, counts, st);
+    else if (kk <= 64) s = launch_egt_batch<2, 32>(b, alpha, counts, st);
+    else if (kk <= 128) s = launch_egt_batch<4, 32>(b, alpha, counts, st);
+    else s = launch_egt_batch<8, 32>(b, alpha, counts, st);
     if (s == EGT_OK) s = csr_batch(b, counts);
     EGT_CUDA_TRY(cudaEventRecord(b->h->ev[5], st));
     cudaFreeAsync(counts, st);
