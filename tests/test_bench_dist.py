@@ -59,3 +59,20 @@ def test_reference_arm_under_torchrun_two_ranks():
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["config"]["n_points"] == 20000
     assert d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_fp32_rates_and_clock_fallback():
+    """The FP32 rate report: operations = evaluations x operations each, over
+    the stage time, against 148 SMs x 128 lanes x 2 at the sampled clock; and
+    the clock sampler reports what it could not sample instead of failing."""
+    sys.path.insert(0, ROOT)
+    import bench
+    r = bench.fp32_rates(10 ** 9, 10.0, 2 * 10 ** 9, 20.0, {"sm_mhz": 1000.0})
+    assert abs(r["knn"]["achieved"] - 0.8) < 1e-9  # 1e9 * 8 / 10 ms = 0.8 TFLOP/s
+    assert abs(r["egt"]["achieved"] - 2.4) < 1e-9  # 2e9 * 24 / 20 ms
+    assert abs(r["knn"]["peak"] - 148 * 128 * 2 * 1e9 / 1e12) < 1e-9
+    assert r["knn"]["frac"] == r["knn"]["achieved"] / r["knn"]["peak"]
+    # no clock sample: the peak falls back to the nominal maximum clock
+    assert abs(bench.fp32_rates(1, 1.0, 1, 1.0, {"sm_mhz": None})["knn"]["peak"] - 148 * 128 * 2 * 1.965e9 / 1e12) < 1e-9
+    clk = bench.ClockSampler(0).stop()
+    assert set(("sm_mhz", "sm_max_mhz", "reasons")) <= set(clk)
