@@ -267,14 +267,13 @@ bool read_binary_triangles(const unsigned char*& p, const unsigned char* end, co
 // lines are located in one pass, then parsed in parallel.  Returns false
 // (p unchanged) when some line does not hold exactly one record; the caller
 // then reads the element sequentially.
-bool read_ascii_lines(const unsigned char*& p, const unsigned char* end, const Element& e, Mesh& m,
-                      const VertexMap* vm) {
-    const char* s = reinterpret_cast<const char*>(p);
-    const char* se = reinterpret_cast<const char*>(end);
-    std::vector<const char*> starts;
-    starts.reserve(e.count + 1);
+// Start of each of the element's `count` lines (blank lines skipped), and
+// the position after the last; false when the data end first.
+bool line_starts(const char* s, const char* se, size_t count, std::vector<const char*>& starts) {
+    starts.clear();
+    starts.reserve(count + 1);
     const char* q = s;
-    for (size_t r = 0; r < e.count; r++) {
+    for (size_t r = 0; r < count; r++) {
         while (q < se && is_space(*q)) q++;  // blank lines and leading spaces
         if (q == se) return false;
         starts.push_back(q);
@@ -282,6 +281,20 @@ bool read_ascii_lines(const unsigned char*& p, const unsigned char* end, const E
         q = nl ? static_cast<const char*>(nl) + 1 : se;
     }
     starts.push_back(q);
+    return true;
+}
+
+// True when only whitespace remains in [c, le).
+bool line_done(const char* c, const char* le) {
+    while (c < le && is_space(*c)) c++;
+    return c == le;
+}
+
+bool read_ascii_lines(const unsigned char*& p, const unsigned char* end, const Element& e, Mesh& m,
+                      const VertexMap* vm) {
+    std::vector<const char*> starts;
+    if (!line_starts(reinterpret_cast<const char*>(p), reinterpret_cast<const char*>(end), e.count, starts))
+        return false;
     const unsigned w = worker_count(e.count);
     std::vector<char> bad(w + 1, 0);
     auto work = [&](unsigned t) {
@@ -294,8 +307,7 @@ bool read_ascii_lines(const unsigned char*& p, const unsigned char* end, const E
                 c = parse_number(c, le, vals[pi]);
                 if (!c) { bad[t] = 1; return; }
             }
-            while (c < le && is_space(*c)) c++;
-            if (c != le) { bad[t] = 1; return; }  // more than one record on the line
+            if (!line_done(c, le)) { bad[t] = 1; return; }  // more than one record on the line
             if (vm) store_vertex(m, *vm, r, vals.data());
         }
     };
@@ -307,7 +319,50 @@ bool read_ascii_lines(const unsigned char*& p, const unsigned char* end, const E
     }
     for (char b : bad)
         if (b) return false;
-    p = reinterpret_cast<const unsigned char*>(q);
+    p = reinterpret_cast<const unsigned char*>(starts.back());
+    return true;
+}
+
+// ASCII face element whose only property is the index list, one face per
+// line: parsed in parallel like read_ascii_lines, keeping the first three
+// indices of each face (0xffffffff for a face with fewer).  Returns false
+// (p and m unchanged) when some line does not hold exactly one face.
+bool read_ascii_faces(const unsigned char*& p, const unsigned char* end, const Element& e, Mesh& m) {
+    std::vector<const char*> starts;
+    if (!line_starts(reinterpret_cast<const char*>(p), reinterpret_cast<const char*>(end), e.count, starts))
+        return false;
+    std::vector<uint32_t> tris(3 * e.count);
+    const unsigned w = worker_count(e.count);
+    std::vector<char> bad(w + 1, 0);
+    auto work = [&](unsigned t) {
+        const size_t b = e.count * t / w, en = e.count * (t + 1) / w;
+        for (size_t r = b; r < en; r++) {
+            const char* c = starts[r];
+            const char* le = starts[r + 1];
+            double v = 0;
+            c = parse_number(c, le, v);
+            if (!c) { bad[t] = 1; return; }
+            const size_t cnt = (size_t)v;
+            uint32_t idx[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
+            for (size_t j = 0; j < cnt; j++) {
+                c = parse_number(c, le, v);
+                if (!c) { bad[t] = 1; return; }
+                if (j < 3) idx[j] = (uint32_t)(int64_t)v;
+            }
+            if (!line_done(c, le)) { bad[t] = 1; return; }
+            tris[3 * r] = idx[0]; tris[3 * r + 1] = idx[1]; tris[3 * r + 2] = idx[2];
+        }
+    };
+    if (w <= 1) work(0);
+    else {
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < w; t++) pool.emplace_back(work, t);
+        for (auto& th : pool) th.join();
+    }
+    for (char b : bad)
+        if (b) return false;
+    m.tris.insert(m.tris.end(), tris.begin(), tris.end());
+    p = reinterpret_cast<const unsigned char*>(starts.back());
     return true;
 }
 
@@ -442,6 +497,8 @@ bool read(const std::string& path, Mesh& m, std::string& err) {
             done = read_binary_triangles(p, end, e, fmt, m);
         } else if (fmt == Fmt::Ascii && !has_list && !e.props.empty()) {
             done = read_ascii_lines(p, end, e, m, vmp);
+        } else if (fmt == Fmt::Ascii && face && il == 0 && e.props.size() == 1) {
+            done = read_ascii_faces(p, end, e, m);
         }
         if (!done) {
             Cursor cur{p, end, fmt};

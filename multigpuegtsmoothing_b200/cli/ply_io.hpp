@@ -11,7 +11,7 @@
 // Large files: the input is mapped into memory, and the common layouts are
 // decoded in parallel on the host cores -- binary elements without lists
 // (fixed-size records), binary face lists that hold only triangles, and ASCII
-// elements without lists written one record per line.  Any other layout (a
+// vertex and face elements written one record per line.  Any other layout (a
 // record spread over several lines, polygons other than triangles, lists
 // inside the vertex element) is read sequentially with the same value
 // conversions, so every layout gives the same result.  The output is laid out

@@ -85,7 +85,7 @@ def test_ply_roundtrip(tmp_path, ascii, big):
     assert np.array_equal(F, tris)
 
 
-@pytest.mark.parametrize("layout", ["le_float", "be_double", "ascii_lines", "ascii_split", "quads"])
+@pytest.mark.parametrize("layout", ["le_float", "be_double", "ascii_lines", "ascii_split", "quads", "ascii_quads"])
 def test_ply_large_inputs(tmp_path, layout):
     """Inputs large enough for the parallel decoders (fixed-size binary
     records, one ASCII record per line, all-triangle face lists), and the
@@ -139,6 +139,9 @@ def test_ply_large_inputs(tmp_path, layout):
         if layout == "ascii_split":  # a record spread over two lines
             lines[n // 2] = lines[n // 2].replace(" ", "\n", 1)
         faces = [f"3 {a} {b} {c}" for a, b, c in tris.tolist()]
+        if layout == "ascii_quads":  # every fifth face a quad: its first three indices are kept
+            faces = [f"4 {a} {b} {c} 0" if j % 5 == 0 else f"3 {a} {b} {c}"
+                     for j, (a, b, c) in enumerate(tris.tolist())]
         src.write_bytes((hdr + "\n".join(lines) + "\n" + "\n".join(faces) + "\n").encode())
     dst = tmp_path / "out.ply"
     subprocess.run([BIN, "--ply-roundtrip", str(src), str(dst)], check=True)
