@@ -90,6 +90,9 @@ typedef struct egt_timings {
                                 with the reference's one-at-a-time insertion rule */
     int64_t knn_evaluations; /* plain kNN: candidate distances evaluated (8 FP32 operations each) */
     int64_t egt_tests;       /* EGT filter: ellipsoid tests evaluated (24 FP32 operations each) */
+    int64_t taubin_tiles;    /* 256-row tiles of the staged Taubin half-step (last CSR smoothed) */
+    int64_t taubin_spill_tiles; /* of those, tiles too large to stage in shared memory, whose rows
+                                   gather their neighbours from global memory */
 } egt_timings;
 
 void egt_default_config(egt_config* cfg);
@@ -184,17 +187,20 @@ egt_status egt_get_timings(egt_handle* h, egt_timings* t);
 egt_status egt_get_csr(egt_handle* h, const int** offsets, const int** cols, int64_t* nnz);
 
 /* Taubin lambda/mu smoothing that allocates no device memory, for callers that
- * cannot allocate: hosts whose single allocator owns all GPU memory, real-time
- * loops that cannot afford cudaMalloc's implicit synchronisation, and code
- * recorded into a CUDA graph.  No counterpart in the reference.
+ * cannot allocate: hosts whose single allocator (a caching allocator or a
+ * pre-sized arena) owns all GPU memory, where a cudaMalloc can fail or
+ * fragment it, and real-time loops that cannot take the device
+ * synchronisation of cudaMalloc/cudaFree.  No counterpart in the reference.
  * pos_in/pos_out: n float4 (x,y,z,w) in device memory (may alias);
  * csr_off [n+1] / csr_col: the neighbourhoods (e.g. from egt_get_csr).
  * The intermediate positions live in a fixed device array of 2^20 float4
- * (16 MB, held by every GPU that loads the library); n above 2^20 is rejected
- * with EGT_ERR_ARG.  The first call on a device resolves that array's device
- * address (cudaGetSymbolAddress), so make it before any stream capture.  All
- * calls share the array: calls that may overlap on the GPU race and must be
- * serialised by the caller. */
+ * (16 MB); n above 2^20 is rejected with EGT_ERR_ARG.  Each call first
+ * resolves that array's device address (cudaGetSymbolAddress) and loads the
+ * half-step kernel on the current device; the first call on a device is the
+ * one that commits the 16 MB (held until the process exits) and the kernel's
+ * module, so make it before any stream capture.  All calls share the array:
+ * calls that may overlap on the GPU race and must be serialised by the
+ * caller. */
 egt_status egt_taubin_noalloc(const float* pos_in, float* pos_out, const int* csr_off, const int* csr_col,
                               int64_t n, int iters, float lambda, float mu, void* stream);
 

@@ -57,7 +57,8 @@ class Timings(C.Structure):
                 ("normals_fp64", C.c_int64), ("msf_edges", C.c_int64), ("components", C.c_int),
                 ("egt_kernel_ms", C.c_float), ("propose_ms", C.c_float), ("box_queries", C.c_int64),
                 ("certified_queries", C.c_int64), ("exact_reruns", C.c_int64),
-                ("knn_evaluations", C.c_int64), ("egt_tests", C.c_int64)]
+                ("knn_evaluations", C.c_int64), ("egt_tests", C.c_int64),
+                ("taubin_tiles", C.c_int64), ("taubin_spill_tiles", C.c_int64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

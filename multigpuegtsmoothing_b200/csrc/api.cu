@@ -466,6 +466,7 @@ egt_status egt_get_timings(egt_handle* h, egt_timings* t) {
     h->tm.exact_reruns = (int64_t)ctr[kCtrExactRerun];
     h->tm.knn_evaluations = h->last_knn_learned ? 0 : (int64_t)ctr[kCtrEvals];
     h->tm.egt_tests = (int64_t)ctr[kCtrEgtTests];
+    h->tm.taubin_spill_tiles = h->tm.taubin_tiles > 0 ? (int64_t)ctr[kCtrSpillTiles] : 0;
     if (h->last_knn_learned) {
         h->tm.propose_ms = elapsed_ms(h->ev[2], h->ev[15]);
         h->tm.box_queries = (int64_t)ctr[kCtrBoxTried];

@@ -111,6 +111,7 @@ constexpr int kCtrExactRerun = 42;  // kNN queries re-searched with the exact in
 constexpr int kCtrWork = 43;        // work queue of the persistent kNN kernels (reset with 42)
 constexpr int kCtrEvals = 44;       // plain kNN: candidate distances evaluated (reset with 42)
 constexpr int kCtrEgtTests = 45;    // EGT filter: ellipsoid tests of the last filter run
+constexpr int kCtrSpillTiles = 46;  // Taubin tiles that gather from global memory (too large to stage)
 
 // One level of the cell hierarchy.  Cells are sorted by key
 // x + y*B + z*B^2; a row is the set of occupied cells sharing (y, z).

@@ -1,19 +1,32 @@
 // Taubin smoothing without any device allocation.
 //
-// Some callers cannot allocate device memory themselves: hosts that hand all
-// of their GPU memory to one allocator of their own and forbid other
-// allocations, real-time loops where the implicit synchronisation of
-// cudaMalloc/cudaFree is not acceptable, and code that records its work into
-// a CUDA graph, where an allocation inside the recorded region is not allowed.
+// Some callers cannot allocate device memory themselves:
+//   * hosts that hand all of their GPU memory to one allocator of their own
+//     (a caching allocator or a pre-sized arena) and forbid other
+//     allocations, where a cudaMalloc can fail or fragment that memory;
+//   * real-time loops (a scanner's or a robot's per-frame smoothing) where
+//     the implicit device synchronisation of cudaMalloc/cudaFree stalls the
+//     loop.
 // egt_taubin_noalloc serves them: the caller passes the input and output
 // positions and the neighbourhood CSR, and the only intermediate buffer the
 // smoothing needs -- the positions between the lambda and the mu half-step --
-// lives in the fixed array below, reserved once per GPU when the library is
-// loaded.
+// lives in the fixed array below.
+//
+// When the memory is committed: CUDA loads a library's kernel modules, and
+// with them their __device__ arrays, lazily -- on a device's first use of
+// them -- unless CUDA_MODULE_LOADING=EAGER asks for it at context creation.
+// Every call therefore starts with a set-up step on the current device that
+// resolves the array's device address (cudaGetSymbolAddress) and loads the
+// half-step kernel's module (cudaFuncGetAttributes), whatever `iters` is.  On
+// the first call on a device this commits the 16 MB array and the module;
+// later calls only look both up.  Make that first call before any stream
+// capture and at a point where the device can still take a 16 MB commitment.
+// Resolving the address on every call (a table lookup once loaded) also keeps
+// it right after cudaDeviceReset, which unloads the module.
 //
 // Limits and sharing rules:
 //   * at most kNoAllocMaxPoints points (larger inputs are rejected);
-//   * every GPU that loads the library holds the 16 MB array until the process
+//   * a device holds the 16 MB array from its first call until the process
 //     exits;
 //   * all calls share the one array: calls that may overlap on the GPU (on
 //     different streams, or from several host threads) race with each other
@@ -21,10 +34,10 @@
 //   * the array keeps the previous call's contents; nothing in it needs to
 //     start at zero, because every half-step writes all n entries before the
 //     next one reads them.
-#include <mutex>
 #include "egt_internal.cuh"
 
 namespace egt {
+egt_status taubin_preload();
 egt_status taubin_launch(const float4* pin, float4* pout, const int* off, const int* col, int n, float scale,
                          cudaStream_t st);
 }
@@ -35,27 +48,14 @@ constexpr int64_t kNoAllocMaxPoints = int64_t(1) << 20;  // 16 MB of float4
 
 static __device__ __align__(256) float4 g_noalloc_scratch[kNoAllocMaxPoints];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-float4* g_scratch_ptr[kMaxDevices] = {};
-
-// Resolves the device address of g_noalloc_scratch on the current device, once
-// per device.  In host code the array's name is only a host-side stand-in:
-// passing it to a kernel directly would fault or use the wrong memory.
-egt_status scratch_for_current_device(float4** out) {
-    int dev = 0;
-    EGT_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) {
-        egt::set_error("egt_taubin_noalloc: device ordinal out of range");
-        return EGT_ERR_ARG;
-    }
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        EGT_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_scratch_ptr[dev] = static_cast<float4*>(p);
-    }
-    *out = g_scratch_ptr[dev];
+// Set-up on the current device: the device address of g_noalloc_scratch (in
+// host code the array's name is only a host-side stand-in, which a kernel
+// must never be given) and the half-step kernel's module.
+egt_status noalloc_setup(float4** out) {
+    void* p = nullptr;
+    EGT_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    EGT_TRY(egt::taubin_preload());
+    *out = static_cast<float4*>(p);
     return EGT_OK;
 }
 
@@ -77,12 +77,13 @@ extern "C" egt_status egt_taubin_noalloc(const float* pos_in, float* pos_out, co
         return EGT_ERR_ARG;
     }
     float4* scratch = nullptr;
-    EGT_TRY(scratch_for_current_device(&scratch));
+    EGT_TRY(noalloc_setup(&scratch));
     cudaStream_t st = (cudaStream_t)stream;
     const float4* in = reinterpret_cast<const float4*>(pos_in);
     float4* out = reinterpret_cast<float4*>(pos_out);
     if (iters == 0) {
-        EGT_CUDA_TRY(cudaMemcpyAsync(out, in, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+        if (in != out)
+            EGT_CUDA_TRY(cudaMemcpyAsync(out, in, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToDevice, st));
         return EGT_OK;
     }
     for (int it = 0; it < iters; it++) {

@@ -274,14 +274,16 @@ __global__ void __launch_bounds__(kTile, 4) k_taubin_tiles(const float4* __restr
 // entry 3g + j of lane l in bits 10j..10j+9 of word soff[w] + 32 g + l;
 // t_soff = soff[0..8] in words, soff[8] the table size).  t_nu = the distinct
 // count, or -1 when the tile does not fit (too many entries, distinct
-// neighbours or slot words): its rows then gather from global memory.
+// neighbours or slot words): its rows then gather from global memory, and the
+// tile is counted in *spilled.
 constexpr int kBuildThreads = 512;
 constexpr int kBuildItems = kTileCap / kBuildThreads;
 
 __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restrict__ off, const int* __restrict__ col,
                                                               int n, int* __restrict__ t_uni,
                                                               uint32_t* __restrict__ t_loc, int* __restrict__ t_nu,
-                                                              int* __restrict__ t_soff) {
+                                                              int* __restrict__ t_soff,
+                                                              unsigned long long* __restrict__ spilled) {
     using Sort = cub::BlockRadixSort<int, kBuildThreads, kBuildItems>;
     using Scan = cub::BlockScan<int, kBuildThreads>;
     __shared__ union {
@@ -301,7 +303,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restr
     const int e_lo = off[base], e_hi = off[last];
     const int cnt = e_hi - e_lo;
     if (cnt > kTileCap) {
-        if (threadIdx.x == 0) t_nu[tile] = -1;
+        if (threadIdx.x == 0) { t_nu[tile] = -1; atomicAdd(spilled, 1ull); }
         return;
     }
     int keys[kBuildItems];
@@ -336,7 +338,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restr
     __syncthreads();
     const int nu = s_nu;
     if (nu > kUCap) {
-        if (threadIdx.x == 0) t_nu[tile] = -1;
+        if (threadIdx.x == 0) { t_nu[tile] = -1; atomicAdd(spilled, 1ull); }
         return;
     }
     for (int i = threadIdx.x; i < cnt; i += kBuildThreads) {
@@ -359,7 +361,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tile_build(const int* __restr
     }
     __syncthreads();
     if (s_soff[kSlices] > kSellWords) {
-        if (threadIdx.x == 0) t_nu[tile] = -1;
+        if (threadIdx.x == 0) { t_nu[tile] = -1; atomicAdd(spilled, 1ull); }
         return;
     }
     for (int u = threadIdx.x; u < nu; u += kBuildThreads) t_uni[(size_t)tile * kUCap + u] = sm.uniq[u];
@@ -467,6 +469,14 @@ __global__ void k_scatter_morton(const float4* __restrict__ mp, const int* __res
 }
 
 }  // namespace
+
+// Loads the module of the general half-step kernel on the current device
+// (CUDA loads kernel modules lazily, on first use, by default).
+egt_status taubin_preload() {
+    cudaFuncAttributes fa{};
+    EGT_CUDA_TRY(cudaFuncGetAttributes(&fa, k_taubin));
+    return EGT_OK;
+}
 
 egt_status taubin_launch(const float4* pin, float4* pout, const int* off, const int* col, int n, float scale,
                          cudaStream_t st) {
@@ -581,9 +591,11 @@ static egt_status morton_prepare(egt_handle* h) {
             EGT_CUDA_TRY(dev_alloc(h, &h->t_soff, sizeof(int) * kSoffWords * tiles));
             h->t_tiles = tiles;
         }
+        EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrSpillTiles, 0, sizeof(unsigned long long), st));
         k_tile_build<<<(unsigned)tiles, kBuildThreads, 0, st>>>(h->m_off, h->m_col, n, h->t_uni, h->t_loc, h->t_nu,
-                                                                 h->t_soff);
+                                                                 h->t_soff, h->d_counters + kCtrSpillTiles);
         EGT_LAUNCH_CHECK();
+        h->tm.taubin_tiles = tiles;
         cudaFreeAsync(kin, st);
         cudaFreeAsync(kout, st);
         cudaFreeAsync(idx, st);

@@ -167,14 +167,91 @@ def test_knn_host_original_order(capi, oracle):
     assert np.array_equal(got, want)
 
 
-def test_superquadrics_4m_digest(capi):
+def angles_deg(a, b):
+    c = np.abs((a * b).sum(0)).clip(0, 1)
+    return np.degrees(np.arccos(c))
+
+
+def test_superquadrics_4m_digest(capi, oracle):
+    """The full 4M-point superquadric workload (k = 40, alpha = 0.65, 300
+    iterations): kNN lists, EGT sets and the smoothed positions of every point
+    against the reference's digests; positions within 1e-6 of the bounding-box
+    diagonal of the FP64 oracle; normals within 0.1 degrees of the FP64 oracle
+    and oriented consistently (the oracle's forest walk leaves them unchanged)."""
     d, m = load("ref_superquadrics_4m")
     dg = m["digests"]
     xyz, _ = regen(m)
     g = cloud(capi, xyz, m["k"])
     assert sha(g.sorted_lists()) == dg["ref_knn_raw"]
-    capi.EGT_CUDA(g).Filter(m["alpha"])
-    assert sha(g.sorted_lists()) == dg["ref_knn_egt"]
+    start = g.sorted_positions()
+    assert sha(start) == dg["ref_pos_in"]
+    egt = capi.EGT_CUDA(g)
+    egt.Filter(m["alpha"])
+    lists = g.sorted_lists()
+    assert sha(lists) == dg["ref_knn_egt"]
+    egt.Taubin(m["iters"], 0.63, -0.64)
+    pos = g.sorted_positions()
+    rows = d["rows"]
+    assert np.array_equal(pos[:, rows], d["ref_pos_out_cols"])
+    assert sha(pos) == dg["ref_pos_out"]
+    scale = float(d["ref_extents"][1]) - float(d["ref_extents"][0])
+    p64 = oracle.taubin_f64(start, lists, m["iters"])
+    assert np.abs(pos - p64).max() * scale <= 1e-6 * bbox_diag(xyz)
+    del p64
+    x, y, z = capi.getOutputPoints(g)
+    assert sha(np.stack([x, y, z])) == dg["ref_out_xyz"]
+    capi.Normal_CUDA(g).GetNormals()
+    got = g.sorted_normals()
+    n64 = oracle.normals(pos, lists, True)
+    assert angles_deg(got, n64).max() < 0.1
+    want, _, nc = oracle.orient(got, lists)
+    assert np.array_equal(want, got)
+    assert g.timings()["components"] == nc
+    g.close()
+
+
+def test_taubin_tile_fallback(capi, oracle):
+    """Tiles too large to stage in shared memory (over 4608 CSR entries or
+    1024 distinct neighbours) gather their neighbours from global memory.  A
+    sphere shell plus a volume blob at alpha = 0.5 keeps up to ~25 neighbours
+    per row in the blob, so a third of the tiles spill and the rest stage:
+    both branches must give the plain one-thread-per-row half-step's result
+    bit for bit (egt_taubin_noalloc runs that kernel) and stay within 1e-6 of
+    the bounding-box diagonal of the FP64 oracle."""
+    import ctypes as C
+    import torch
+
+    rng = np.random.default_rng(1)
+    xyz = np.concatenate([datagen.sphere_cloud(20000, 0.005, 41),
+                          (rng.random((10000, 3)) * 0.6 - 0.3).astype(np.float32)])
+    iters = 20
+    g = cloud(capi, xyz, 40)
+    egt = capi.EGT_CUDA(g)
+    egt.Filter(0.5)
+    start = g.sorted_positions()
+    lists = g.sorted_lists()
+    n = start.shape[1]
+    off_p, col_p, nnz = C.c_void_p(), C.c_void_p(), C.c_int64()
+    capi._check(capi.lib().egt_get_csr(g.handle, C.byref(off_p), C.byref(col_p), C.byref(nnz)))
+    pin = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    pin[:, :3] = torch.from_numpy(start.T.copy()).cuda()
+    pout = torch.empty_like(pin)
+    torch.cuda.synchronize()
+    st = capi.lib().egt_taubin_noalloc(C.c_void_p(pin.data_ptr()), C.c_void_p(pout.data_ptr()), off_p, col_p, n,
+                                       iters, 0.63, -0.64, None)
+    assert st == 0, capi.lib().egt_last_error()
+    torch.cuda.synchronize()
+    plain = pout[:, :3].cpu().numpy().T.copy()
+    egt.Taubin(iters, 0.63, -0.64)
+    t = g.timings()
+    assert t["taubin_tiles"] == (n + 255) // 256
+    assert 0 < t["taubin_spill_tiles"] < t["taubin_tiles"], t
+    pos = g.sorted_positions()
+    assert np.array_equal(pos, plain)
+    scale = g.GetMaxExtent() - g.GetMinExtent()
+    p64 = oracle.taubin_f64(start, lists, iters)
+    assert np.abs(pos - p64).max() * scale <= 1e-6 * bbox_diag(xyz)
+    g.close()
 
 
 def test_chunked_knn_host_matches_search_then_copy(capi):

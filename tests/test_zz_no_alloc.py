@@ -1,12 +1,14 @@
 """egt_taubin_noalloc: Taubin smoothing for callers that cannot allocate device
-memory (their own allocator owns the GPU, they run real-time loops that cannot
-take cudaMalloc's synchronisation, or they record their work into a CUDA graph).
+memory -- a host whose own allocator owns all GPU memory, or a real-time loop
+that cannot take cudaMalloc's device synchronisation.
 
 The entry point is called through the C ABI on device buffers the test owns
-and must reproduce the regular egt_taubin result of a provider handle, on two
-calls in a row (the shared scratch array keeps the first call's contents, which
-the second call must not depend on).  The file is named so that pytest
-collects it last; it needs nothing from the other tests.
+and must reproduce the regular egt_taubin result of a provider handle bit for
+bit (both accumulate every row in list order with the same arithmetic), and
+stay within 1e-6 of the bounding-box diagonal of the FP64 oracle, on two calls
+in a row (the shared scratch array keeps the first call's contents, which the
+second call must not depend on).  The file is named so that pytest collects it
+last; it needs nothing from the other tests.
 """
 import ctypes as C
 
@@ -19,7 +21,7 @@ from multigpuegtsmoothing_b200 import datagen
 pytestmark = pytest.mark.gpu
 
 
-def test_taubin_noalloc_matches_handle_taubin(capi):
+def test_taubin_noalloc_matches_handle_taubin(capi, oracle):
     import torch
 
     xyz = datagen.sphere_cloud(30000, 0.005, 41)
@@ -29,6 +31,7 @@ def test_taubin_noalloc_matches_handle_taubin(capi):
     egt = capi.EGT_CUDA(g)
     egt.Filter(0.65)
     start = g.sorted_positions()                      # (3, n) before smoothing
+    lists = g.sorted_lists()
     off_p, col_p, nnz = C.c_void_p(), C.c_void_p(), C.c_int64()
     capi._check(capi.lib().egt_get_csr(g.handle, C.byref(off_p), C.byref(col_p), C.byref(nnz)))
     n = start.shape[1]
@@ -51,10 +54,17 @@ def test_taubin_noalloc_matches_handle_taubin(capi):
     want = g.sorted_positions()
     scale = g.GetMaxExtent() - g.GetMinExtent()
     tol = 1e-6 * bbox_diag(xyz)
+    p64 = oracle.taubin_f64(start, lists, iters, lam, mu)
     for got in results:
-        assert np.isfinite(got).all()
-        assert np.abs(got - want).max() * scale <= tol
+        assert np.array_equal(got, want)
+        assert np.abs(got - p64).max() * scale <= tol
     assert np.array_equal(results[0], results[1])
+    # zero iterations on aliased buffers: nothing to do, the positions stay
+    st = capi.lib().egt_taubin_noalloc(C.c_void_p(pout.data_ptr()), C.c_void_p(pout.data_ptr()), off_p, col_p, n,
+                                       0, lam, mu, None)
+    assert st == 0, capi.lib().egt_last_error()
+    torch.cuda.synchronize()
+    assert np.array_equal(pout[:, :3].cpu().numpy().T, results[1])
 
 
 def test_taubin_noalloc_rejects_oversize(capi):
