@@ -263,6 +263,41 @@ def cpu_baseline(xyz, k, budget_s=20.0):
             "build_s": tb, "query_s_sample": tq}
 
 
+def cpu_stages(pos, knn_lists, egt_lists, smoothed, alpha, iters, taubin_sample_iters=2):
+    """The later stages of the oracle on the host cores, on the inputs the GPU
+    pipeline gives each stage (sorted space): the EGT filter over every row,
+    Taubin for `taubin_sample_iters` iterations scaled to `iters`, the FP32
+    normals and the spanning-forest orientation over every point."""
+    from oracle import pyoracle
+    out = {"cores": pyoracle.num_threads(), "kind": "port"}
+    t = time.perf_counter()
+    pyoracle.egt(pos, knn_lists, alpha)
+    out["egt_filter_ms"] = (time.perf_counter() - t) * 1e3
+    t = time.perf_counter()
+    pyoracle.taubin_f32(pos, egt_lists, taubin_sample_iters)
+    out[f"taubin_{iters}_iters_ms"] = (time.perf_counter() - t) * 1e3 * iters / taubin_sample_iters
+    t = time.perf_counter()
+    nrm = pyoracle.normals(smoothed, egt_lists, False)
+    out["normals_ms"] = (time.perf_counter() - t) * 1e3
+    t = time.perf_counter()
+    pyoracle.orient(nrm, egt_lists)
+    out["orientation_ms"] = (time.perf_counter() - t) * 1e3
+    out["sample"] = (f"every row of the {pos.shape[1]}-point workload; Taubin {taubin_sample_iters} iterations "
+                     f"scaled to {iters}")
+    return out
+
+
+def reference_gpu_stages():
+    """The unmodified reference's per-stage GPU times, as tests/golden/time_reference.py
+    last measured them on a B200 (None when the file is absent)."""
+    p = os.path.join(ROOT, "tests", "golden", "ref_gpu_stages.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    d["source"] = "tests/golden/time_reference.py (unmodified reference built for sm_100a by oracle/ref/Makefile)"
+    return d
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -315,21 +350,30 @@ def learned_vs_plain(capi):
     g.GRIDCUDAKNNSELF_COMPACT(k)
     ref = g.sorted_lists()
     p.tune(g)
-    plain_ms, learned_ms = [], []
+    ring = capi.GridStructure(xyz, config=capi.default_config(knn_mode=2))
+    ring_ms, learned_ms, select_ms = [], [], []
     for _ in range(3):
-        g.GRIDCUDAKNNSELF_COMPACT(k)
-        plain_ms.append(g.timings()["knn_ms"])
+        ring.GRIDCUDAKNNSELF_COMPACT(k)
+        ring_ms.append(ring.timings()["knn_ms"])
         g.GRIDCUDAKNNSELF_LEARNED(k, p)
         learned_ms.append(g.timings()["knn_ms"])
-    t = g.timings()
-    same = bool(np.array_equal(g.sorted_lists(), ref))
+        t = g.timings()
+        g.GRIDCUDAKNNSELF_COMPACT(k)
+        select_ms.append(g.timings()["knn_ms"])
+    same = bool(np.array_equal(ring.sorted_lists(), ref))
+    g.GRIDCUDAKNNSELF_LEARNED(k, p)
+    same = same and bool(np.array_equal(g.sorted_lists(), ref))
+    ring.close()
     n = xyz.shape[0]
     out = {"workload": f"sheets {n} points, 1000:1 density range, k={k}",
-           "plain_ms": min(plain_ms), "learned_ms": min(learned_ms),
-           "plain_mqueries_s": n / min(plain_ms) / 1e3, "learned_mqueries_s": n / min(learned_ms) / 1e3,
-           "speedup": min(plain_ms) / min(learned_ms), "lists_identical": same, "tau": p.tau,
+           "plain": "the reference's ring expansion (EGT_KNN_RING, k_knn_plain)",
+           "plain_ms": min(ring_ms), "learned_ms": min(learned_ms),
+           "plain_mqueries_s": n / min(ring_ms) / 1e3, "learned_mqueries_s": n / min(learned_ms) / 1e3,
+           "speedup": min(ring_ms) / min(learned_ms), "lists_identical": same, "tau": p.tau,
            "box_queries_frac": t["box_queries"] / n, "certified_frac": t["certified_queries"] / n,
-           "train_loss_first_last": [float(losses[0]), float(losses[-1])]}
+           "train_loss_first_last": [float(losses[0]), float(losses[-1])],
+           "block_selection_ms": min(select_ms), "block_selection_mqueries_s": n / min(select_ms) / 1e3,
+           "block_selection_note": "egt_knn's default path (EGT_KNN_PLAIN) on the same cloud, same lists"}
     g.close()
     p.close()
     return out
@@ -377,6 +421,39 @@ def batched(capi, iters: int = 150, alpha: float = 0.65):
             "taubin_point_iters_per_s": n * iters / (t["taubin_ms"] * 1e-3),
             "clouds_bit_identical_to_single": f"{same}/{len(sample)}",
             "knn_chunk": t["knn_chunk"], "taubin_mode": t["taubin_mode"]}
+
+
+def pipeline_configs(capi):
+    """Stage times of this build on the two small single-cloud workloads, the
+    35,947-point noisy sphere (k=40, alpha 0.65, 150 iterations, normals) and
+    the 131,072-vertex torus mesh (1-ring capped at 40, alpha 1e-8, 150
+    iterations): each pipeline runs once to warm up, then once timed (CUDA
+    events per stage, egt_get_timings)."""
+    from multigpuegtsmoothing_b200 import datagen
+    out = {}
+    sphere = datagen.sphere_cloud()
+    xyz_t, tris = datagen.torus_mesh()
+    for name in ("sphere_c1", "torus_c2"):
+        for rep in range(2):
+            if name == "sphere_c1":
+                g = capi.GridStructure(sphere)
+                g.GRIDCUDAKNNSELF_COMPACT(40)
+                capi.EGT_CUDA(g).PerformSmoothing(150, 0.63, -0.64, 0.65)
+                capi.Normal_CUDA(g).GetNormals()
+            else:
+                g = capi.GridMeshCuda(xyz_t, tris)
+                g.GetNeighborsFromTriangles(40)
+                capi.EGT_CUDA(g).PerformSmoothing(150, 0.63, -0.64, 1e-8)
+            capi.getOutputPoints(g)
+            t = g.timings()
+            g.close()
+        rec = {"points": int(t.get("points", 0)) or (sphere.shape[0] if name == "sphere_c1" else xyz_t.shape[0]),
+               "grid_knn_ms": t["grid_ms"] + t["knn_ms"], "egt_taubin_ms": t["egt_ms"] + t["taubin_ms"],
+               "output_ms": t["output_ms"]}
+        if name == "sphere_c1":
+            rec["normals_orient_ms"] = t["normals_ms"] + t["orient_ms"]
+        out[name] = rec
+    return out
 
 
 def run_b200(args, world, rank, local):
@@ -440,6 +517,8 @@ def run_b200(args, world, rank, local):
     for warm in (True, False):
         g.UpdatePointsDevice(xyz_dev.data_ptr())
         g.GRIDCUDAKNNSELF_COMPACT(K)
+        if not warm and rank == 0 and world == 1 and not args.no_cpu_baseline:
+            knn_lists, start_pos = g.sorted_lists(), g.sorted_positions()
         egt.Filter(ALPHA)
         tmf = g.timings()
         if warm:
@@ -448,7 +527,15 @@ def run_b200(args, world, rank, local):
     t_egt, t_egt_kernel = tmf["egt_ms"], tmf["egt_kernel_ms"]
     nnz = tmf["csr_nnz"]
     knn_evals, egt_tests = tm["knn_evaluations"], tmf["egt_tests"]
-    egt.Taubin(ITERS)  # warm-up (graph capture path)
+    # first Taubin call on this CSR: Morton relabelling, per-tile tables and the
+    # graph capture of the 2*ITERS half-steps, then the replay
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    egt.Taubin(ITERS)
+    torch.cuda.synchronize()
+    taubin_first_wall_ms = (time.perf_counter() - w0) * 1e3
+    taubin_first_dev_ms = g.timings()["taubin_ms"]
+    spill = g.timings()
     torch.cuda.synchronize()
     ta, tb_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = max(1, min(args.steps, 3))
@@ -465,6 +552,11 @@ def run_b200(args, world, rank, local):
     # normals (PCA, FP64 re-solve of near-degenerate gaps) + spanning-tree orientation
     capi.Normal_CUDA(g).GetNormals()
     tmn = g.timings()
+    stages_cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        stages_cpu = cpu_stages(start_pos, knn_lists, g.sorted_lists(), g.sorted_positions(), ALPHA, ITERS)
+        del knn_lists, start_pos
+    configs = pipeline_configs(capi) if rank == 0 and not args.no_configs else None
 
     # e2e through the C ABI with pinned host buffers
     host_xyz = torch.from_numpy(xyz).pin_memory()
@@ -497,6 +589,10 @@ def run_b200(args, world, rank, local):
                           "taubin_300_iters": taubin_ms, "normals": tmn["normals_ms"],
                           "orientation": tmn["orient_ms"],
                           "note": "egt_filter..orientation: second pass of the pipeline on a warm memory pool"},
+            "taubin_first_call": {"device_ms": taubin_first_dev_ms, "wall_ms": taubin_first_wall_ms,
+                                  "note": "first egt_taubin on a new CSR: Morton relabelling, per-tile tables, "
+                                          "graph capture, then the 300 iterations; taubin_300_iters replays the "
+                                          "cached graph"},
             "taubin_iters_per_s": ITERS / (taubin_ms * 1e-3),
             "taubin_roofline": {"bound": "hbm", "achieved": taubin_gbs, "peak": peak, "unit": "GB/s",
                                 "frac": taubin_gbs / peak, "peak_kind": peak_kind,
@@ -512,14 +608,24 @@ def run_b200(args, world, rank, local):
             "fp32": fp32_rates(knn_evals, knn_ms, egt_tests, t_egt_kernel, clk),
             "gpu_launches": int(launches),
             "clocks": clk,
-            "knn_stats": {"invalid_queries": tm["invalid_queries"], "levels_used": tm["levels_used"]},
+            "knn_stats": {"invalid_queries": tm["invalid_queries"], "levels_used": tm["levels_used"],
+                          "ring_search_queries": tm["knn_fallback"], "exact_reruns": tm["exact_reruns"],
+                          "note": "ring_search_queries: rows the block selection could not certify "
+                                  "(equal distances, ...), searched by the reference's ring expansion"},
+            "taubin_tiles": {"tiles": spill["taubin_tiles"], "spilled": spill["taubin_spill_tiles"]},
         }
+        if configs is not None:
+            line["configs"] = configs
+        ref_gpu = reference_gpu_stages()
+        if ref_gpu is not None:
+            line["reference_gpu"] = ref_gpu
         if not args.no_learned:
             line["learned_vs_plain"] = learned_vs_plain(capi)
         if not args.no_batched:
             line["batched"] = batched(capi)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(xyz, K)
+            line["cpu_baseline"]["stages"] = stages_cpu
         print(json.dumps(line), flush=True)
     g.close()
 
@@ -533,6 +639,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal comparison")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-clouds workload")
+    ap.add_argument("--no-configs", action="store_true", help="skip the 36K-sphere and torus-mesh stage times")
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="workload size override (profiling a smaller case of the same step)")
     args = ap.parse_args()

@@ -43,8 +43,9 @@ typedef struct egt_proposal egt_proposal;
 #define EGT_PROPOSAL_CLASSES 16
 #define EGT_PROPOSAL_PARAMS 1872
 
-#define EGT_KNN_PLAIN 0
-#define EGT_KNN_LEARNED 1
+#define EGT_KNN_PLAIN 0    /* block selection, certified rows; the ring search for the rest */
+#define EGT_KNN_LEARNED 1  /* proposal-driven box search, certified rows; the ring search for the rest */
+#define EGT_KNN_RING 2     /* the reference's ring expansion alone, query by query */
 
 /* Tunables.  Defaults reproduce the reference CLI (main.cpp:108-116). */
 typedef struct egt_config {
@@ -53,8 +54,9 @@ typedef struct egt_config {
     int bucket_count;        /* level-0 buckets per axis (1024) */
     float threshold;         /* GRIDCUDAKNNSELF_COMPACT thres before scaling (1e8) */
     int max_points_in_cell;  /* MAX_PNTS_IN_CUBE (100000): larger cells invalidate a query */
-    int knn_mode;            /* EGT_KNN_PLAIN, or EGT_KNN_LEARNED: egt_knn uses the proposal
-                                attached with egt_attach_proposal */
+    int knn_mode;            /* EGT_KNN_PLAIN (default), EGT_KNN_RING, or EGT_KNN_LEARNED: egt_knn
+                                uses the proposal attached with egt_attach_proposal.  All three
+                                give identical lists. */
     int warps_per_block;     /* kNN/EGT launch shape (0 = autotuned default) */
     float normals_gap_tol;   /* FP64 eigensolve when (l1-l0) < tol*l2 (0.1; 0 = FP32 only) */
 } egt_config;
@@ -93,6 +95,8 @@ typedef struct egt_timings {
     int64_t taubin_tiles;    /* 256-row tiles of the staged Taubin half-step (last CSR smoothed) */
     int64_t taubin_spill_tiles; /* of those, tiles too large to stage in shared memory, whose rows
                                    gather their neighbours from global memory */
+    int64_t knn_fallback;    /* plain kNN: queries the block-selection search could not certify
+                                (equal distances, oversized cells, ...) and the ring search ran */
 } egt_timings;
 
 void egt_default_config(egt_config* cfg);
@@ -117,8 +121,14 @@ egt_status egt_create_mesh(const float* xyz_host, int64_t n, const uint32_t* tri
  * hierarchy are rebuilt, previous lists/CSR/normals are invalidated. */
 egt_status egt_update_points_device(egt_handle* h, const float* xyz_dev, void* stream);
 
-/* GridStructure::GRIDCUDAKNNSELF_COMPACT(k, thres) (GridKNNCuda.cu:2322-2634). */
+/* GridStructure::GRIDCUDAKNNSELF_COMPACT(k, thres) (GridKNNCuda.cu:2322-2634),
+ * with the handle's threshold (egt_config.threshold, or egt_set_threshold). */
 egt_status egt_knn(egt_handle* h, int k, void* stream);
+/* The thres argument of GRIDCUDAKNNSELF_COMPACT / GRIDCUDAKNNCompact
+ * (GridKNNCuda.cu:2324-2325, :1667-1668): the admission threshold of the
+ * following searches on h, in the reference's units (scaled by the
+ * normalisation extent and squared on the device).  thres > 0. */
+egt_status egt_set_threshold(egt_handle* h, float thres, void* stream);
 /* GridMeshCuda::GetNeighborsFromTriangles(k) (GridMeshCuda1.cu:416-511). */
 egt_status egt_mesh_1ring(egt_handle* h, int k, void* stream);
 
@@ -180,6 +190,19 @@ egt_status egt_orient_kruskal(const int* knn, float* nx, float* ny, float* nz, c
 
 /* Device pointers behind the KNNInterface getters. */
 egt_status egt_get_views(egt_handle* h, egt_views* views);
+/* Hands back what a KNNInterface consumer left in the provider's slots, as the
+ * reference's consumers leave it (EGT_CUDA::PerformSmoothing writes smoothed
+ * positions through GetRefPointsX/Y/Z()[0] and may swap those pointers,
+ * EGT_CUDA.cu:591-632; calculateEGG_GKNN writes -1 into the lists in place,
+ * EGT_CUDA.cu:172-189): x, y, z are the arrays now in the slots (device SoA,
+ * sorted space, normalised; the handle's own views or a consumer's buffers),
+ * copied into the handle; the lists are taken as rewritten, so later stages
+ * rebuild their neighbourhoods from them. */
+egt_status egt_commit_views(egt_handle* h, const float* x, const float* y, const float* z, void* stream);
+/* cudaFree for a device buffer a KNNInterface consumer swapped into a
+ * provider slot: the provider frees whatever its slots hold at destruction
+ * (GridKNNCuda.cu:1005-1021). */
+egt_status egt_free_device(void* p);
 /* Per-stage device timings of the last calls (filled when the stream is synced). */
 egt_status egt_get_timings(egt_handle* h, egt_timings* t);
 /* Sorted-space EGT-filtered neighbourhoods as CSR (device pointers, valid

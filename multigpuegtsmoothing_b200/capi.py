@@ -58,7 +58,7 @@ class Timings(C.Structure):
                 ("egt_kernel_ms", C.c_float), ("propose_ms", C.c_float), ("box_queries", C.c_int64),
                 ("certified_queries", C.c_int64), ("exact_reruns", C.c_int64),
                 ("knn_evaluations", C.c_int64), ("egt_tests", C.c_int64),
-                ("taubin_tiles", C.c_int64), ("taubin_spill_tiles", C.c_int64)]
+                ("taubin_tiles", C.c_int64), ("taubin_spill_tiles", C.c_int64), ("knn_fallback", C.c_int64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -106,6 +106,9 @@ def lib() -> C.CDLL:
             "egt_output_device": (i32, [vp, vp, vp, vp, vp]),
             "egt_get_knn_host": (i32, [vp, vp, vp]),
             "egt_get_views": (i32, [vp, C.POINTER(Views)]),
+            "egt_commit_views": (i32, [vp, vp, vp, vp, vp]),
+            "egt_free_device": (i32, [vp]),
+            "egt_set_threshold": (i32, [vp, f32, vp]),
             "egt_get_timings": (i32, [vp, C.POINTER(Timings)]),
             "egt_get_csr": (i32, [vp, hp, hp, C.POINTER(C.c_int64)]),
             "egt_copy_to_host": (i32, [vp, vp, vp, i64]),
@@ -298,9 +301,11 @@ class GridStructure(_Handle):
         """Rebuild normalisation, cell sort and hierarchy for new device positions (same n)."""
         _check(lib().egt_update_points_device(self.handle, C.c_void_p(device_ptr), self.stream))
 
-    def GRIDCUDAKNNSELF_COMPACT(self, k: int, thres: float = 1e8):
-        if np.float32(thres) != np.float32(1e8):
-            raise EgtError(-2, "thres is fixed at creation (config.threshold)")
+    def GRIDCUDAKNNSELF_COMPACT(self, k: int, thres: Optional[float] = None):
+        """GRIDCUDAKNNSELF_COMPACT(k, thres): thres (the reference's units) is set
+        on the handle when given; otherwise the handle's threshold stays."""
+        if thres is not None:
+            _check(lib().egt_set_threshold(self.handle, float(thres), self.stream))
         _check(lib().egt_knn(self.handle, int(k), self.stream))
 
     def knn_host(self, k: int, out: Optional[np.ndarray] = None) -> np.ndarray:

@@ -51,7 +51,7 @@ void free_handle(egt_handle* h) {
     for (int L = 0; L < kMaxLevels; L++) {
         F(h->lv[L].order); F(h->lv[L].cell_start); F(h->lv[L].cell_x); F(h->lv[L].row_range);
     }
-    F(h->lists); F(h->kth); F(h->qlevel); F(h->pclass); F(h->csr_off); F(h->csr_col); F(h->tris); F(h->nrm);
+    F(h->lists); F(h->kth); F(h->qlevel); F(h->knn_fb); F(h->pclass); F(h->csr_off); F(h->csr_col); F(h->tris); F(h->nrm);
     F(h->d_counters); F(h->scratch.ptr);
     if (h->taubin_exec) cudaGraphExecDestroy(h->taubin_exec);
     F(h->m_perm); F(h->m_inv); F(h->m_p); F(h->m_pb); F(h->m_off); F(h->m_col);
@@ -126,6 +126,10 @@ egt_status create_common(const float* xyz, bool xyz_on_device, int64_t n, const 
         return EGT_ERR_ARG;
     }
     if (cfg.max_points_in_cell < 1) { set_error("max_points_in_cell must be >= 1"); return EGT_ERR_ARG; }
+    if (cfg.knn_mode != EGT_KNN_PLAIN && cfg.knn_mode != EGT_KNN_LEARNED && cfg.knn_mode != EGT_KNN_RING) {
+        set_error("knn_mode must be EGT_KNN_PLAIN, EGT_KNN_LEARNED or EGT_KNN_RING");
+        return EGT_ERR_ARG;
+    }
     EGT_CUDA_TRY(cudaSetDevice(cfg.device));
     EGT_TRY(warm_pool(cfg.device));
     egt_handle* h = new egt_handle();
@@ -222,6 +226,14 @@ egt_status egt_update_points_device(egt_handle* h, const float* xyz_dev, void* s
 }
 
 int64_t egt_kernel_launches(void) { return g_launches; }
+
+egt_status egt_set_threshold(egt_handle* h, float thres, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (!(thres > 0.0f)) { set_error("egt_set_threshold: thres must be > 0"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    return set_threshold(h, thres);
+}
 
 egt_status egt_knn(egt_handle* h, int k, void* stream) {
     EGT_TRY(check_handle(h));
@@ -414,6 +426,49 @@ egt_status egt_get_knn_host(egt_handle* h, int* knn_host, void* stream) {
     return s;
 }
 
+}  // extern "C"
+
+namespace {
+// Positions a KNNInterface consumer left in the provider's slots (device SoA,
+// sorted space) into the handle's float4 array; the slot arrays are copied
+// into the handle's SoA mirror when they are not that mirror.
+__global__ void k_commit_positions(const float* __restrict__ x, const float* __restrict__ y,
+                                   const float* __restrict__ z, int64_t n, float4* __restrict__ p4, float* hx,
+                                   float* hy, float* hz) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float vx = x[i], vy = y[i], vz = z[i];
+    float4 p = p4[i];
+    p.x = vx; p.y = vy; p.z = vz;
+    p4[i] = p;
+    if (x != hx) hx[i] = vx;
+    if (y != hy) hy[i] = vy;
+    if (z != hz) hz[i] = vz;
+}
+}  // namespace
+
+extern "C" {
+
+egt_status egt_commit_views(egt_handle* h, const float* x, const float* y, const float* z, void* stream) {
+    EGT_TRY(check_handle(h));
+    if (!x || !y || !z) { set_error("egt_commit_views: null position array"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(h->cfg.device));
+    bind_stream(h, stream);
+    const unsigned T = 256;
+    k_commit_positions<<<(unsigned)((h->n + T - 1) / T), T, 0, h->stream>>>(x, y, z, h->n, h->p4, h->x, h->y,
+                                                                             h->z);
+    EGT_LAUNCH_CHECK();
+    // the lists may have been rewritten in place: neighbourhoods are rebuilt
+    // from them by the next stage that needs them
+    h->have_csr = false;
+    return EGT_OK;
+}
+
+egt_status egt_free_device(void* p) {
+    if (p) EGT_CUDA_TRY(cudaFree(p));
+    return EGT_OK;
+}
+
 egt_status egt_get_views(egt_handle* h, egt_views* v) {
     EGT_TRY(check_handle(h));
     if (!v) { set_error("egt_get_views: null output"); return EGT_ERR_ARG; }
@@ -464,6 +519,7 @@ egt_status egt_get_timings(egt_handle* h, egt_timings* t) {
     h->tm.msf_edges = (int64_t)ctr[kCtrMsf];
     h->tm.components = (int)ctr[kCtrComps];
     h->tm.exact_reruns = (int64_t)ctr[kCtrExactRerun];
+    h->tm.knn_fallback = h->last_knn_learned ? 0 : (int64_t)ctr[kCtrSelFallback];
     h->tm.knn_evaluations = h->last_knn_learned ? 0 : (int64_t)ctr[kCtrEvals];
     h->tm.egt_tests = (int64_t)ctr[kCtrEgtTests];
     h->tm.taubin_spill_tiles = h->tm.taubin_tiles > 0 ? (int64_t)ctr[kCtrSpillTiles] : 0;

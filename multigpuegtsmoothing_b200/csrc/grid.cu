@@ -63,6 +63,13 @@ __global__ void k_finalize_norm(const uint32_t* acc, float eps, float thres0, in
     *out = finalize_norm(acc, eps, thres0, n);
 }
 
+// GRIDCUDAKNNSELF_COMPACT's threshold scaling (GridKNNCuda.cu:2324-2325):
+// thres /= (maxExtent - minExtent); thres *= thres.
+__global__ void k_set_thres(float thres0, NormParams* np) {
+    float t = __fdiv_rn(thres0, __fsub_rn(np->mx, np->mn));
+    np->thres = __fmul_rn(t, t);
+}
+
 // normalize_points (GridKNNCuda.cu:840-849) + get_buckets_no_binary at B=1024
 // (GridKNNCuda.cu:74-88): normalised float4 in original order and the key.
 __global__ void k_normalize_key(const float* __restrict__ xyz, int64_t n, const NormParams* __restrict__ np,
@@ -276,6 +283,13 @@ egt_status build_grid(egt_handle* h, const float* xyz, int levels) {
     EGT_TRY(s);
     EGT_CUDA_TRY(cudaMemcpyAsync(&h->norm, h->d_norm, sizeof(NormParams), cudaMemcpyDeviceToHost, st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[1], st));
+    return EGT_OK;
+}
+
+egt_status set_threshold(egt_handle* h, float thres) {
+    k_set_thres<<<1, 1, 0, h->stream>>>(thres, h->d_norm);
+    EGT_LAUNCH_CHECK();
+    h->cfg.threshold = thres;
     return EGT_OK;
 }
 

@@ -33,6 +33,7 @@
 #include "egt_internal.cuh"
 #include "knn_common.cuh"
 #include "knn_search.cuh"
+#include "knn_select.cuh"
 #include "proposal.cuh"
 
 namespace egt {
@@ -53,8 +54,9 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_plain(KnnArgs a
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const NormParams np = *a.np;
     unsigned evals = 0;  // candidate distances this lane evaluated
-    for (int q0 = claim(a, lane); q0 < a.n; q0 = claim(a, lane)) {
-        const int q1 = min(q0 + a.chunk, a.n);
+    const int n = launch_size(a);
+    for (int q0 = claim(a, lane, n); q0 < n; q0 = claim(a, lane, n)) {
+        const int q1 = min(q0 + a.chunk, n);
         for (int jq = q0; jq < q1; jq++) {
             const int q = a.qmap ? a.qmap[jq] : jq;
             const float4 pq = a.p4[q];
@@ -72,6 +74,44 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_plain(KnnArgs a
     if (lane == 0 && evals) atomicAdd(&a.counters[kCtrEvals], (unsigned long long)evals);
     __syncthreads();
     if (threadIdx.x == 0 && s_rerun) atomicAdd(&a.counters[kCtrExactRerun], (unsigned long long)s_rerun);
+}
+
+// Block-selection search (knn_select.cuh), persistent like k_knn_plain.
+// Queries it cannot certify are appended to fb (count *nfb) for the ring
+// search.
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_select(KnnArgs a, int* __restrict__ fb,
+                                                                         unsigned long long* __restrict__ nfb) {
+    __shared__ SelScratch s_sc[kWarps];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const NormParams np = *a.np;
+    // every distance admitted (the under-full rule then always continues)
+    const bool usable = np.thres > 4.0f;
+    const int n = launch_size(a);
+    unsigned evals = 0;
+    int gstart = 0, maxlevel = 0;
+    for (int q0 = claim(a, lane, n); q0 < n; q0 = claim(a, lane, n)) {
+        const int q1 = min(q0 + a.chunk, n);
+        for (int jq = q0; jq < q1; jq++) {
+            const int q = a.qmap ? a.qmap[jq] : jq;
+            SelOut r{false, 0, 0.0f};
+            if (usable) r = sel_query(a, np, q, a.p4[q], lane, s_sc[w], gstart, evals);
+            if (lane == 0) {
+                if (r.ok) {
+                    if (a.kth_out) a.kth_out[q] = r.kth;
+                    if (a.qlevel) a.qlevel[q] = (uint8_t)r.reached;
+                    maxlevel = max(maxlevel, r.reached);
+                } else {
+                    fb[atomicAdd(nfb, 1ull)] = q;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
+    if (lane == 0) {
+        if (evals) atomicAdd(&a.counters[kCtrEvals], (unsigned long long)evals);
+        if (maxlevel) atomicMax(&a.counters[kCtrMaxLevel], (unsigned long long)maxlevel);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -453,8 +493,9 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_learned(KnnArgs
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const NormParams np = *a.np;
-    for (int q0 = claim(a, lane); q0 < a.n; q0 = claim(a, lane)) {
-        const int q1 = min(q0 + a.chunk, a.n);
+    const int n = launch_size(a);
+    for (int q0 = claim(a, lane, n); q0 < n; q0 = claim(a, lane, n)) {
+        const int q1 = min(q0 + a.chunk, n);
         for (int jq = q0; jq < q1; jq++) {
             const int q = a.qmap ? a.qmap[jq] : jq;
             const float4 pq = a.p4[q];
@@ -571,8 +612,9 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_query(KnnArgs a
     const NormParams np = *a.np;
     const float thres_lt = nextafterf(np.thres, 0.0f);  // d <= thres_lt  <=>  d < thres
     const float ab = __fsub_rn(np.b, np.a);
-    for (int q0 = claim(a, lane); q0 < a.n; q0 = claim(a, lane)) {
-        const int q1 = min(q0 + a.chunk, a.n);
+    const int n = launch_size(a);
+    for (int q0 = claim(a, lane, n); q0 < n; q0 = claim(a, lane, n)) {
+        const int q1 = min(q0 + a.chunk, n);
         for (int jq = q0; jq < q1; jq++) {
             const int row = a.qmap[jq];
             const float4 pq = qpos[row];
@@ -714,6 +756,7 @@ static egt_status knn_prepare(egt_handle* h, int k, KnnArgs* a) {
     }
     if (!h->kth) EGT_CUDA_TRY(dev_alloc(h, &h->kth, sizeof(float) * n));
     if (!h->qlevel) EGT_CUDA_TRY(dev_alloc(h, &h->qlevel, n));
+    if (!h->knn_fb) EGT_CUDA_TRY(dev_alloc(h, &h->knn_fb, sizeof(int) * n));
     h->have_csr = false;
     a->p4 = h->p4;
     a->np = h->d_norm;
@@ -743,14 +786,69 @@ static egt_status knn_launch(const KnnArgs& a, cudaStream_t st) {
     return EGT_OK;
 }
 
+// Device words of one exact search over a.n queries: the selection kernel's
+// work counter, its list of uncertified queries (room for a.n) and their
+// count, and the ring search's work counter over that list.  All counters
+// must be zero.
+struct SearchSlots {
+    unsigned long long* sel_work;
+    unsigned long long* nfb;
+    unsigned long long* fb_work;
+    int* fb;
+};
+
+template <typename K>
+static egt_status select_blocks(K kernel, unsigned* out) {
+    static std::mutex mu;
+    static std::map<int, unsigned> cache;
+    int dev = 0;
+    EGT_CUDA_TRY(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(dev);
+        if (it != cache.end()) { *out = it->second; return EGT_OK; }
+    }
+    int sms = 0, per = 0;
+    EGT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    EGT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kWarps * 32, 0));
+    *out = (unsigned)std::max(1, sms * std::max(per, 1));
+    std::lock_guard<std::mutex> lock(mu);
+    cache[dev] = *out;
+    return EGT_OK;
+}
+
+// The exact plain search of a.n queries: the block-selection kernel, then the
+// ring search over the queries it could not certify (lists of more than
+// kSelMaxK neighbours run the ring search alone).
+static egt_status knn_search(const KnnArgs& a, const SearchSlots& sl, bool ring_only, cudaStream_t st) {
+    if (ring_only || a.k > kSelMaxK) return knn_launch(a, st);
+    KnnArgs as = a;
+    as.work = sl.sel_work;
+    unsigned G = 0;
+    EGT_TRY(select_blocks(k_knn_select, &G));
+    const int64_t need = ((int64_t)a.n + kWarps * kChunk - 1) / (kWarps * kChunk);
+    G = (unsigned)std::max<int64_t>(1, std::min<int64_t>(G, need));
+    k_knn_select<<<G, kWarps * 32, 0, st>>>(as, sl.fb, sl.nfb);
+    EGT_LAUNCH_CHECK();
+    KnnArgs af = a;
+    af.qmap = sl.fb;
+    af.n_dev = sl.nfb;
+    af.work = sl.fb_work;
+    return knn_launch(af, st);
+}
+
 egt_status run_knn(egt_handle* h, int k) {
     cudaStream_t st = h->stream;
     KnnArgs a;
     EGT_TRY(knn_prepare(h, k, &a));
+    EGT_TRY(level_maxpop(h));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, 3 * sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrSelWork, 0, 3 * sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
-    EGT_TRY(knn_launch(a, st));
+    const SearchSlots sl{h->d_counters + kCtrSelWork, h->d_counters + kCtrSelFallback, h->d_counters + kCtrFbWork,
+                         h->knn_fb};
+    EGT_TRY(knn_search(a, sl, h->cfg.knn_mode == EGT_KNN_RING, st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[3], st));
     return EGT_OK;
 }
@@ -772,6 +870,15 @@ __global__ void k_chunk_keys(const int* __restrict__ perm, int n, ChunkBounds cb
     while ((int)c + 1 < cb.count && r >= cb.end[c]) c++;
     key[s] = c;
     idx[s] = s;
+}
+
+// Adds the per-chunk counts of uncertified queries to the handle's counter.
+__global__ void k_sum_counts(const unsigned long long* __restrict__ v, int m, unsigned long long* __restrict__ out) {
+    unsigned long long t = 0;
+    for (int i = threadIdx.x; i < m; i += 32) t += v[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) *out += t;
 }
 
 // Rows of queries qmap[0..m) in original order and ids (GetKNNIndexes layout).
@@ -829,8 +936,10 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
     EGT_CUDA_TRY(cudaMallocAsync((void**)&idx, sizeof(int) * n, st));
     EGT_CUDA_TRY(cudaMallocAsync((void**)&qmap, sizeof(int) * n, st));
     EGT_CUDA_TRY(cudaMallocAsync((void**)&out, sizeof(int) * (size_t)n * k, st));
-    EGT_CUDA_TRY(cudaMallocAsync((void**)&work, sizeof(unsigned long long) * chunks, st));
-    EGT_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long) * chunks, st));
+    // per chunk: ring-search work counter, selection work counter, uncertified count, their ring-search counter
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&work, sizeof(unsigned long long) * 4 * chunks, st));
+    EGT_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long) * 4 * chunks, st));
+    EGT_TRY(level_maxpop(h));
     const unsigned T = 256;
     k_chunk_keys<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(h->perm, n, cb, key, idx);
     EGT_LAUNCH_CHECK();
@@ -842,6 +951,7 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrEvals, 0, sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrSelFallback, 0, sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
     // streams: [0] = h->stream, [1] = a second search stream, [2] = copies
     cudaStream_t ss[3] = {st, nullptr, nullptr};
@@ -866,7 +976,9 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
         ac.qmap = qmap + r0;
         ac.n = m;
         ac.work = work + c;
-        s = knn_launch(ac, cs);
+        // the chunk's uncertified queries go to fb[r0, r0 + m)
+        const SearchSlots sl{work + chunks + c, work + 2 * chunks + c, work + 3 * chunks + c, h->knn_fb + r0};
+        s = knn_search(ac, sl, h->cfg.knn_mode == EGT_KNN_RING, cs);
         if (s != EGT_OK) break;
         const int64_t cnt = (int64_t)m * k;
         k_rows_original<<<(unsigned)((cnt + T - 1) / T), T, 0, cs>>>(h->lists, h->perm, qmap + r0, m, k, out);
@@ -882,6 +994,11 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
     // join: the first stream waits for the second search stream, then ends the timing
     if (s == EGT_OK) fail(cudaEventRecord(ev[2 * chunks + 1], ss[1]), "cudaEventRecord");
     if (s == EGT_OK) fail(cudaStreamWaitEvent(st, ev[2 * chunks + 1], 0), "cudaStreamWaitEvent");
+    if (s == EGT_OK) {
+        k_sum_counts<<<1, 32, 0, st>>>(work + 2 * chunks, chunks, h->d_counters + kCtrSelFallback);
+        count_launch();
+        fail(cudaGetLastError(), "k_sum_counts");
+    }
     if (s == EGT_OK) fail(cudaEventRecord(h->ev[3], st), "cudaEventRecord");
     fail(cudaStreamSynchronize(ss[2]), "copy stream");
     fail(cudaStreamSynchronize(ss[1]), "search stream");
@@ -991,6 +1108,7 @@ egt_status run_knn_learned(egt_handle* h, int k, const egt_proposal* p) {
     }
     if (!h->kth) EGT_CUDA_TRY(dev_alloc(h, &h->kth, sizeof(float) * n));
     if (!h->qlevel) EGT_CUDA_TRY(dev_alloc(h, &h->qlevel, n));
+    if (!h->knn_fb) EGT_CUDA_TRY(dev_alloc(h, &h->knn_fb, sizeof(int) * n));
     h->have_csr = false;
     EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
     EGT_TRY(level_maxpop(h));

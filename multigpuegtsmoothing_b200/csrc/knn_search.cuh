@@ -21,7 +21,11 @@ struct KnnArgs {
     unsigned long long* __restrict__ counters;
     const int* __restrict__ qmap = nullptr;  // query j of a launch is qmap[j] (nullptr: j)
     unsigned long long* __restrict__ work = nullptr;  // work counter (nullptr: counters[kCtrWork])
+    const unsigned long long* __restrict__ n_dev = nullptr;  // launch size on the device (nullptr: n)
 };
+
+// Queries of a launch: n, or the count a preceding kernel left on the device.
+__device__ __forceinline__ int launch_size(const KnnArgs& a) { return a.n_dev ? (int)*a.n_dev : a.n; }
 
 constexpr int kWarps = 8;
 // The search kernels are latency-bound: keep four blocks (32 warps) resident
@@ -329,10 +333,10 @@ __device__ __forceinline__ void write_query(const KnnArgs& a, int q, const WarpL
 constexpr int kChunk = 4;
 
 // Next chunk of queries for the calling warp (uniform); >= n when done.
-__device__ __forceinline__ int claim(const KnnArgs& a, int lane) {
+__device__ __forceinline__ int claim(const KnnArgs& a, int lane, int n) {
     unsigned long long q0 = 0;
     if (lane == 0) q0 = atomicAdd(a.work ? a.work : &a.counters[kCtrWork], (unsigned long long)a.chunk);
-    return (int)min(__shfl_sync(0xffffffffu, q0, 0), (unsigned long long)a.n);
+    return (int)min(__shfl_sync(0xffffffffu, q0, 0), (unsigned long long)n);
 }
 
 }  // namespace

@@ -760,11 +760,11 @@ void orc_extents(const float* xyz, int n, float* ext) { cube_extents(xyz, n, ext
 //   perm [n], ext [2], level [n] (optional): level at which the query stopped
 //   (0..7, 8 = ran out of levels), kth [n] (optional): k-th distance (1e10 if < k).
 // Returns the number of invalid queries.
-int orc_knn(const float* xyz, int n, int k, int* lists, float* pos, int* perm, float* ext,
+int orc_knn(const float* xyz, int n, int k, float thres_in, int* lists, float* pos, int* perm, float* ext,
             int* level, float* kth, long long* visited_total) {
     Grid g;
     build_grid(xyz, n, g, kLevels);
-    float thres = 1e8f;
+    float thres = thres_in;  // GRIDCUDAKNNSELF_COMPACT(k, thres), GridKNNCuda.cu:2324-2325
     thres /= (g.mx - g.mn);
     thres *= thres;
     int invalid_count = 0;
@@ -1310,6 +1310,85 @@ void orc_bruteforce(const float* pos, int n, int k, int* lists, float* dists) {
             }
         }
     }
+}
+
+// Checks the certification rule of the block-selection kNN (product kernel
+// k_knn_select) against the reference's ring search (knn_query): for every
+// query the cloud's exact k+1 nearest points are found by brute force, and the
+// query is "certified" when
+//   (1) the k+1 smallest distances are pairwise distinct,
+//   (2) the first step s of the ring search (0 = own level-0 cell, s >= 1 =
+//       the ring at level s-1) whose face test (decide_more, GridKNNCuda.cu:
+//       694-741) stops on the k-th distance exists,
+//   (3) the k nearest lie inside the block that step s has visited (level-0
+//       cell keys),
+//   (4) no cell of the levels visited up to step s holds MAX_PNTS_IN_CUBE
+//       points or more (GridKNNCuda.cu:672, 685).
+// stats[0] = certified rows, stats[1] = certified rows whose ring-search list
+// differs from the k nearest in ascending order (the rule says 0), stats[2] =
+// certified rows whose ring-search stop level differs from step s.
+void orc_select_check(const float* xyz, int n, int k, long long* stats) {
+    Grid g;
+    build_grid(xyz, n, g, kLevels);
+    float thres = 1e8f;
+    thres /= (g.mx - g.mn);
+    thres *= thres;
+    int maxpop[kLevels];
+    for (int L = 0; L < kLevels; L++) {
+        maxpop[L] = 0;
+        for (size_t c = 0; c + 1 < g.lv[L].start.size(); c++)
+            maxpop[L] = std::max(maxpop[L], g.lv[L].start[c + 1] - g.lv[L].start[c]);
+    }
+    long long certified = 0, wrong = 0, wrong_level = 0;
+#pragma omp parallel reduction(+ : certified, wrong, wrong_level)
+    {
+        std::vector<std::pair<float, int>> c((size_t)n);
+        std::vector<float> dist(k);
+        std::vector<int> idx(k);
+#pragma omp for schedule(dynamic, 64)
+        for (int q = 0; q < n; q++) {
+            int m = 0;
+            for (int p = 0; p < n; p++)
+                if (p != q) c[m++] = {dist3(g.x[q], g.y[q], g.z[q], g.x[p], g.y[p], g.z[p]), p};
+            if (m < k + 1) continue;
+            std::partial_sort(c.begin(), c.begin() + k + 1, c.begin() + m);
+            bool ok = true;
+            for (int j = 1; j <= k; j++) ok &= c[j - 1].first < c[j].first;
+            if (!ok) continue;
+            const float T = c[k - 1].first;
+            int sf = -1;
+            for (int st = 0; st <= kLevels; st++) {
+                const int Ls = st == 0 ? 0 : st - 1, o = st == 0 ? 0 : 1;
+                if (!decide_more(g, q, Ls, o, k, k, T, thres)) { sf = st; break; }
+            }
+            if (sf < 0) continue;
+            for (int j = 0; j < k && ok; j++) {
+                const int p = c[j].second;
+                if (sf == 0) {
+                    ok = g.cx[p] == g.cx[q] && g.cy[p] == g.cy[q] && g.cz[p] == g.cz[q];
+                } else {
+                    const int L = sf - 1;
+                    ok = std::abs((g.cx[p] >> L) - (g.cx[q] >> L)) <= 1 &&
+                         std::abs((g.cy[p] >> L) - (g.cy[q] >> L)) <= 1 &&
+                         std::abs((g.cz[p] >> L) - (g.cz[q] >> L)) <= 1;
+                }
+            }
+            for (int L = 0; L <= std::max(sf - 1, 0) && ok; L++) ok = maxpop[L] < kMaxPointsInCube;
+            if (!ok) continue;
+            certified++;
+            int counter;
+            bool invalid;
+            long long visited = 0;
+            const int reached = knn_query(g, q, k, thres, dist.data(), idx.data(), counter, invalid, visited);
+            bool same = !invalid;
+            for (int j = 0; j < k && same; j++) same = idx[j] == c[j].second;
+            if (!same) wrong++;
+            if (reached != std::max(sf - 1, 0)) wrong_level++;
+        }
+    }
+    stats[0] = certified;
+    stats[1] = wrong;
+    stats[2] = wrong_level;
 }
 
 // orient_kruskal (MST.cpp:399-423) on host normals, in place; key32 as in

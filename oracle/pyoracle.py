@@ -33,7 +33,7 @@ def lib():
         L.orc_num_threads.restype = i32
         L.orc_extents.argtypes = [vp, i32, vp]
         L.orc_knn.restype = i32
-        L.orc_knn.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp, vp, vp]
+        L.orc_knn.argtypes = [vp, i32, i32, f32, vp, vp, vp, vp, vp, vp, vp]
         L.orc_knn_query.restype = i32
         L.orc_knn_query.argtypes = [vp, i32, vp, i32, i32, f32, vp, vp]
         L.orc_mesh_1ring.argtypes = [vp, i32, vp, i32, i32, vp, vp, vp, vp]
@@ -46,6 +46,7 @@ def lib():
         L.orc_orient_kruskal.argtypes = [vp, C.c_int64, i32, i32, vp, vp, vp, i32]
         L.orc_output.argtypes = [vp, vp, vp, i32, vp]
         L.orc_bruteforce.argtypes = [vp, i32, i32, vp, vp]
+        L.orc_select_check.argtypes = [vp, i32, i32, vp]
         L.orc_knn_timed.argtypes = [vp, i32, i32, i32, vp, vp]
         L.orc_proposal_data.restype = i32
         L.orc_proposal_data.argtypes = [vp, i32, i32, vp, vp]
@@ -63,7 +64,7 @@ def num_threads() -> int:
     return lib().orc_num_threads()
 
 
-def knn(xyz: np.ndarray, k: int):
+def knn(xyz: np.ndarray, k: int, thres: float = 1e8):
     """Reference grid kNN.  Returns dict(lists, pos, perm, ext, level, kth, invalid, visited)."""
     xyz = np.ascontiguousarray(xyz, dtype=np.float32)
     n = xyz.shape[0]
@@ -74,7 +75,7 @@ def knn(xyz: np.ndarray, k: int):
     level = np.empty(n, np.int32)
     kth = np.empty(n, np.float32)
     visited = C.c_longlong(0)
-    inv = lib().orc_knn(_p(xyz), n, k, _p(lists), _p(pos), _p(perm), _p(ext), _p(level), _p(kth),
+    inv = lib().orc_knn(_p(xyz), n, k, float(thres), _p(lists), _p(pos), _p(perm), _p(ext), _p(level), _p(kth),
                         C.byref(visited))
     return dict(lists=lists, pos=pos, perm=perm, ext=ext, level=level, kth=kth, invalid=inv,
                 visited=visited.value)
@@ -178,6 +179,16 @@ def bruteforce(pos: np.ndarray, k: int):
     d = np.empty((n, k), np.float32)
     lib().orc_bruteforce(_p(pos), n, k, _p(lists), _p(d))
     return lists, d
+
+
+def select_check(xyz: np.ndarray, k: int):
+    """Certification rule of the block-selection kNN against the ring search
+    (brute force; small clouds): (certified rows, certified rows whose ring-search
+    list is not the k nearest in order, certified rows with another stop level)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+    st = np.zeros(3, np.int64)
+    lib().orc_select_check(_p(xyz), xyz.shape[0], k, _p(st))
+    return tuple(int(v) for v in st)
 
 
 def knn_timed(xyz: np.ndarray, k: int, stride: int):

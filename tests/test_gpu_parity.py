@@ -110,6 +110,44 @@ def test_knn_superquadric_subset(capi, oracle):
     assert np.array_equal(g.sorted_lists(), oracle.egt(r["pos"], r["lists"], 0.65))
 
 
+def _cloud_case(case):
+    rng = np.random.default_rng(5)
+    if case == "sphere":
+        return datagen.sphere_cloud(60000, 0.005, 51)
+    if case == "superquadrics":
+        return datagen.superquadrics(300_000, seed=52)
+    if case == "clusters":
+        return np.concatenate([rng.normal(c, s, (20000, 3)) for c, s in
+                               [((0, 0, 0), 0.002), ((0.5, 0.1, 0), 0.05), ((1, 1, 1), 0.3)]]).astype(np.float32)
+    d, _ = load("ref_lattice" if case == "lattice" else "ref_dups")
+    return d["in_xyz"]
+
+
+@pytest.mark.parametrize("case,k", [("sphere", 40), ("superquadrics", 40), ("superquadrics", 64), ("clusters", 20),
+                                    ("clusters", 95), ("dups", 5), ("lattice", 8), ("sphere", 1), ("sphere", 96)])
+def test_select_matches_ring_search(capi, case, k):
+    """egt_knn's block selection (EGT_KNN_PLAIN) against the reference's ring
+    expansion run query by query (EGT_KNN_RING): identical lists, invalid rows
+    and deepest level.  Certified rows come from the selection kernel, the rest
+    (ties, oversized cells, k > 95) from the ring search."""
+    xyz = _cloud_case(case)
+    g = cloud(capi, xyz, k)
+    r = cloud(capi, xyz, k, capi.default_config(knn_mode=2))
+    assert np.array_equal(g.sorted_lists(), r.sorted_lists())
+    t, tr = g.timings(), r.timings()
+    assert t["invalid_queries"] == tr["invalid_queries"]
+    assert t["levels_used"] == tr["levels_used"]
+    n = xyz.shape[0]
+    if k > 95:
+        assert t["knn_fallback"] == 0 and t["knn_evaluations"] == tr["knn_evaluations"]
+    elif case in ("sphere", "superquadrics", "clusters"):
+        assert t["knn_fallback"] < 0.05 * n, t["knn_fallback"]
+    # the lists in original order through the chunked host path too
+    assert np.array_equal(g.knn_host(k), r.GetKNNIndexes())
+    g.close()
+    r.close()
+
+
 def test_edge_cases(capi, oracle):
     # a single point: no neighbours, the row is invalid
     g = cloud(capi, np.zeros((1, 3), np.float32), 4)

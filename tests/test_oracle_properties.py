@@ -25,6 +25,35 @@ def test_grid_knn_is_exact(oracle, n, k, seed):
             assert set(got.tolist()) == set(bl[q].tolist())
 
 
+@pytest.mark.parametrize("case", ["sphere", "superquadrics", "clusters", "lattice", "dups"])
+def test_select_certification_rule(oracle, case):
+    """The rule the block-selection kNN certifies its rows by: where the cloud's
+    k+1 nearest distances are distinct, the ring search's face test stops on
+    the k-th of them at some step, the k nearest lie in that step's block and no
+    visited level has an oversized cell, the ring search's list is exactly the k
+    nearest in ascending order and it stops at that step (brute force over the
+    whole cloud, every row)."""
+    import os
+    from golden_util import load
+    k = 16
+    if case == "sphere":
+        xyz = datagen.sphere_cloud(6000, 0.01, 21)
+    elif case == "superquadrics":
+        xyz = datagen.superquadrics(8000, seed=22)
+    elif case == "clusters":
+        rng = np.random.default_rng(23)
+        xyz = np.concatenate([rng.normal(c, s, (2000, 3)) for c, s in
+                              [((0, 0, 0), 0.002), ((0.5, 0.1, 0), 0.05), ((1, 1, 1), 0.3)]]).astype(np.float32)
+    else:
+        d, _ = load("ref_lattice" if case == "lattice" else "ref_dups")
+        xyz = d["in_xyz"]
+    n = xyz.shape[0]
+    certified, wrong, wrong_level = oracle.select_check(xyz, k)
+    assert wrong == 0 and wrong_level == 0
+    if case not in ("lattice", "dups"):  # exact ties everywhere: duplicate points, lattice spacings
+        assert certified > 0.5 * n
+
+
 def test_small_n_all_invalid(oracle):
     # n <= k: no query can collect k neighbours, every row is invalid
     xyz = datagen.sphere_cloud(20, 0.01, 4)
