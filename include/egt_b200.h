@@ -209,6 +209,16 @@ egt_status egt_get_timings(egt_handle* h, egt_timings* t);
  * until the next call on the handle): offsets [n+1], cols [nnz]. */
 egt_status egt_get_csr(egt_handle* h, const int** offsets, const int** cols, int64_t* nnz);
 
+/* One half-step of taubin_step_GKNN (EGT_CUDA.cu:229-276) over rows
+ * [0, rows) of a CSR -- the per-GPU step of the reference's partitioned
+ * smoothing (EGT_CUDA.cu:559-633), whose halo exchange the caller does:
+ * pos_in: device float4 (x,y,z,w) positions indexed by csr_col (row i's own
+ * position is pos_in[i]; entries past the rows hold the halo), pos_out: rows
+ * float4 (w copied), not aliasing pos_in; scale: lambda or mu.  Allocates
+ * nothing. */
+egt_status egt_taubin_halfstep(const float* pos_in, float* pos_out, const int* csr_off, const int* csr_col,
+                               int64_t rows, float scale, int device, void* stream);
+
 /* Taubin lambda/mu smoothing that allocates no device memory, for callers that
  * cannot allocate: hosts whose single allocator (a caching allocator or a
  * pre-sized arena) owns all GPU memory, where a cudaMalloc can fail or

@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
             "egt_update_points_device": (i32, [vp, vp, vp]),
             "egt_kernel_launches": (i64, []),
             "egt_taubin_noalloc": (i32, [vp, vp, vp, vp, i64, i32, f32, f32, vp]),
+            "egt_taubin_halfstep": (i32, [vp, vp, vp, vp, i64, f32, i32, vp]),
             "egt_destroy": (None, [vp]),
             "egt_proposal_create": (i32, [i32, i32, C.c_uint64, hp]),
             "egt_proposal_destroy": (None, [vp]),

@@ -449,6 +449,20 @@ __global__ void k_commit_positions(const float* __restrict__ x, const float* __r
 
 extern "C" {
 
+egt_status egt_taubin_halfstep(const float* pos_in, float* pos_out, const int* csr_off, const int* csr_col,
+                               int64_t rows, float scale, int device, void* stream) {
+    if (rows < 0 || rows > (int64_t)0x7fffffff) { set_error("egt_taubin_halfstep: rows out of range"); return EGT_ERR_ARG; }
+    if (rows == 0) return EGT_OK;
+    if (!pos_in || !pos_out || !csr_off || !csr_col) {
+        set_error("egt_taubin_halfstep: null pointer argument");
+        return EGT_ERR_ARG;
+    }
+    if (pos_in == pos_out) { set_error("egt_taubin_halfstep: pos_in and pos_out must not alias"); return EGT_ERR_ARG; }
+    EGT_CUDA_TRY(cudaSetDevice(device));
+    return taubin_launch(reinterpret_cast<const float4*>(pos_in), reinterpret_cast<float4*>(pos_out), csr_off,
+                         csr_col, (int)rows, scale, (cudaStream_t)stream);
+}
+
 egt_status egt_commit_views(egt_handle* h, const float* x, const float* y, const float* z, void* stream) {
     EGT_TRY(check_handle(h));
     if (!x || !y || !z) { set_error("egt_commit_views: null position array"); return EGT_ERR_ARG; }

@@ -232,6 +232,8 @@ egt_status run_egt(egt_handle* h, float alpha);
 egt_status ensure_csr(egt_handle* h);
 egt_status csr_nnz(egt_handle* h, int64_t* out);
 egt_status run_taubin(egt_handle* h, int iters, float lambda, float mu);
+egt_status taubin_launch(const float4* pin, float4* pout, const int* off, const int* col, int n, float scale,
+                         cudaStream_t st);
 egt_status run_normals(egt_handle* h);
 egt_status run_orient(egt_handle* h);
 egt_status run_orient_kruskal(const int* knn, float* nrm, int n, int k, int k_use, cudaStream_t st);

@@ -1036,6 +1036,34 @@ void orc_taubin_f32(float* pos, int n, int k, const int* lists, int iters, float
     if (in != pos) std::memcpy(pos, in, sizeof(float) * 3 * (size_t)n);
 }
 
+// One half-step of taubin_step_GKNN (EGT_CUDA.cu:229-276) over rows [0, rows)
+// of a CSR: row i's own position is in[i] and its neighbours are in[col[e]],
+// e in [off[i], off[i+1]), list order; positions are float4 (x, y, z, w) as
+// the GPU keeps them, m of them (rows <= m).  out: rows float4 (w copied).
+// The per-rank step of a row-partitioned smoothing, whose halo positions sit
+// in in[rows..m).
+void orc_taubin_rows_f32(const float* in, int m, int rows, const int* off, const int* col, float scale,
+                         float* out) {
+    (void)m;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < rows; i++) {
+        const float x1 = in[4 * (size_t)i], y1 = in[4 * (size_t)i + 1], z1 = in[4 * (size_t)i + 2];
+        float cx = 0, cy = 0, cz = 0, sum = 0;
+        for (int e = off[i]; e < off[i + 1]; e++) {
+            const size_t q = 4 * (size_t)col[e];
+            const float x2 = in[q], y2 = in[q + 1], z2 = in[q + 2];
+            float w = std::exp(-dist3_taubin(x1, y1, z1, x2, y2, z2));
+            cx = acc(cx, w, x2 - x1); cy = acc(cy, w, y2 - y1); cz = acc(cz, w, z2 - z1);
+            sum += w;
+        }
+        if (sum == 0.0f) sum = 1e-8f;
+        out[4 * (size_t)i] = x1 + scale * cx / sum;
+        out[4 * (size_t)i + 1] = y1 + scale * cy / sum;
+        out[4 * (size_t)i + 2] = z1 + scale * cz / sum;
+        out[4 * (size_t)i + 3] = in[4 * (size_t)i + 3];
+    }
+}
+
 // Same iteration in double precision (the FP64 oracle).
 void orc_taubin_f64(double* pos, int n, int k, const int* lists, int iters, double lambda, double mu) {
     std::vector<double> tmp(3 * (size_t)n);

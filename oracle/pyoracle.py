@@ -40,6 +40,7 @@ def lib():
         L.orc_egt.argtypes = [vp, i32, i32, vp, f32, vp]
         L.orc_taubin_f32.argtypes = [vp, i32, i32, vp, i32, f32, f32]
         L.orc_taubin_f64.argtypes = [vp, i32, i32, vp, i32, C.c_double, C.c_double]
+        L.orc_taubin_rows_f32.argtypes = [vp, i32, i32, vp, vp, f32, vp]
         L.orc_normals.argtypes = [vp, i32, i32, vp, i32, vp]
         L.orc_orient.restype = i32
         L.orc_orient.argtypes = [i32, i32, vp, vp, vp]
@@ -121,6 +122,18 @@ def taubin_f32(pos: np.ndarray, lists: np.ndarray, iters: int, lam=0.63, mu=-0.6
     n, k = lists.shape
     lib().orc_taubin_f32(_p(p), n, k, _p(lists), iters, lam, mu)
     return p
+
+
+def taubin_rows_f32(pos4: np.ndarray, rows: int, off: np.ndarray, col: np.ndarray, scale: float) -> np.ndarray:
+    """One FP32 half-step over rows [0, rows) of a CSR whose columns index the
+    (m, 4) float32 positions pos4 (own position of row i = pos4[i]); returns
+    the (rows, 4) new positions."""
+    pos4 = np.ascontiguousarray(pos4, dtype=np.float32)
+    off = np.ascontiguousarray(off, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    out = np.empty((rows, 4), np.float32)
+    lib().orc_taubin_rows_f32(_p(pos4), pos4.shape[0], rows, _p(off), _p(col), float(scale), _p(out))
+    return out
 
 
 def taubin_f64(pos: np.ndarray, lists: np.ndarray, iters: int, lam=0.63, mu=-0.64) -> np.ndarray:

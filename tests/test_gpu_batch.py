@@ -2,11 +2,14 @@
 
 Every cloud of a batch must give exactly what its own GridStructure gives
 through the same calls: kNN lists, EGT-filtered lists and smoothed positions,
-bit for bit, whatever tuning the batch runs with.
+bit for bit, whatever tuning the batch runs with; and what the CPU oracle (the
+restatement of the reference) gives for that cloud alone: identical kNN and EGT
+lists, positions within 1e-6 of the bounding-box diagonal of the FP64 oracle.
 """
 import numpy as np
 import pytest
 
+from golden_util import bbox_diag
 from multigpuegtsmoothing_b200 import datagen
 
 pytestmark = pytest.mark.gpu
@@ -88,6 +91,48 @@ def test_batch_autotuned_run(capi, reference):
     t = b.timings()
     assert t["knn_chunk"] in (1, 2, 4, 8, 16) and t["taubin_mode"] in (0, 1)
     b.close()
+
+
+def _original(perm, lists):
+    """Sorted-space lists of the oracle in original ids and row order."""
+    out = np.full_like(lists, -1)
+    out[perm] = np.where(lists >= 0, perm[np.clip(lists, 0, None)], -1)
+    return out
+
+
+def test_batch_clouds_match_oracle(capi, oracle):
+    """Clouds of every k in {10, 20, 40} (noisy spheres, the vertices of a
+    noisy torus, superquadrics), a lattice (exact ties) and a cloud with
+    duplicated points, batched together, each checked against the oracle run on
+    that cloud alone."""
+    g = np.random.default_rng(9)
+    clouds = [(datagen.sphere_cloud(9000, 0.005, 91), 10), (datagen.sphere_cloud(25000, 0.005, 92), 40),
+              (datagen.torus_mesh(128, 96)[0], 20),
+              (datagen.superquadrics(30000, seed=94), 40)]
+    t = np.arange(14, dtype=np.float32)
+    clouds.append((np.stack(np.meshgrid(t, t, t, indexing="ij"), -1).reshape(-1, 3), 20))
+    a = g.random((5000, 3), dtype=np.float32)
+    clouds.append((np.concatenate([a, a[:500]]), 10))
+    iters, alpha = 30, 0.65
+    b = capi.Batch(clouds)
+    b.knn()
+    knn = [b.knn_host(c) for c in range(len(clouds))]
+    b.filter(alpha)
+    filt = [b.knn_host(c) for c in range(len(clouds))]
+    b.taubin(iters)
+    out = b.output()
+    b.close()
+    for c, (xyz, k) in enumerate(clouds):
+        r = oracle.knn(xyz, k)
+        perm = r["perm"]
+        assert np.array_equal(knn[c], _original(perm, r["lists"])), c
+        e = oracle.egt(r["pos"], r["lists"], alpha)
+        assert np.array_equal(filt[c], _original(perm, e)), c
+        p64 = oracle.taubin_f64(r["pos"], e, iters)
+        lo, hi = float(r["ext"][0]), float(r["ext"][1])
+        want = np.empty((xyz.shape[0], 3))
+        want[perm] = (p64 * (hi - lo) + lo).T
+        assert np.abs(out[c] - want).max() <= 1e-6 * bbox_diag(xyz), c
 
 
 def test_batch_bad_arguments(capi):

@@ -58,9 +58,8 @@ def test_reference_consumers_on_cloud_provider(consumers):
     assert np.array_equal(pos, d["ref_pos_out"])
     assert np.array_equal(out, d["ref_out_xyz"])
     assert np.array_equal(out_lib, d["ref_out_xyz"])
-    c = np.abs((nrm * d["ref_normals"]).sum(0)).clip(0, 1)
-    assert np.degrees(np.arccos(c)).max() < 1e-3
-    assert ((nrm * d["ref_normals"]).sum(0) > 0).all()
+    # the reference's normal code on the same positions and lists: its normals exactly
+    assert np.array_equal(nrm, d["ref_normals"])
 
 
 def test_reference_consumers_on_mesh_provider(consumers):
@@ -81,7 +80,7 @@ def test_reference_consumers_on_mesh_provider(consumers):
     assert np.array_equal(out_lib, d["ref_out_xyz"])
 
 
-@pytest.mark.parametrize("k,frac", [(16, 0.5), (40, 1.0)])
+@pytest.mark.parametrize("k,frac", [(16, 1.0), (40, 1.2)])
 def test_finite_threshold_matches_oracle(capi, oracle, k, frac):
     """GRIDCUDAKNNSELF_COMPACT(k, thres) with thres a fraction of the typical
     k-th neighbour distance: admission is cut at thres, under-full lists continue

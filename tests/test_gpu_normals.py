@@ -16,6 +16,12 @@ pytestmark = pytest.mark.gpu
 
 
 def angles_deg(a, b):
+    """Unsigned angles between unit columns, in float64 (float32 arccos near 1
+    reads ~0.03 degrees for identical vectors)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    a = a / np.linalg.norm(a, axis=0)
+    b = b / np.linalg.norm(b, axis=0)
     c = np.abs((a * b).sum(0)).clip(0, 1)
     return np.degrees(np.arccos(c))
 
