@@ -43,9 +43,9 @@ typedef struct egt_proposal egt_proposal;
 #define EGT_PROPOSAL_CLASSES 16
 #define EGT_PROPOSAL_PARAMS 1872
 
-#define EGT_KNN_PLAIN 0    /* block selection, certified rows; the ring search for the rest */
+#define EGT_KNN_PLAIN 0    /* the reference's ring expansion, one warp per query */
 #define EGT_KNN_LEARNED 1  /* proposal-driven box search, certified rows; the ring search for the rest */
-#define EGT_KNN_RING 2     /* the reference's ring expansion alone, query by query */
+#define EGT_KNN_SELECT 2   /* block selection, certified rows; the ring search for the rest */
 
 /* Tunables.  Defaults reproduce the reference CLI (main.cpp:108-116). */
 typedef struct egt_config {
@@ -54,7 +54,7 @@ typedef struct egt_config {
     int bucket_count;        /* level-0 buckets per axis (1024) */
     float threshold;         /* GRIDCUDAKNNSELF_COMPACT thres before scaling (1e8) */
     int max_points_in_cell;  /* MAX_PNTS_IN_CUBE (100000): larger cells invalidate a query */
-    int knn_mode;            /* EGT_KNN_PLAIN (default), EGT_KNN_RING, or EGT_KNN_LEARNED: egt_knn
+    int knn_mode;            /* EGT_KNN_PLAIN (default), EGT_KNN_SELECT, or EGT_KNN_LEARNED: egt_knn
                                 uses the proposal attached with egt_attach_proposal.  All three
                                 give identical lists. */
     int warps_per_block;     /* kNN/EGT launch shape (0 = autotuned default) */
@@ -95,7 +95,7 @@ typedef struct egt_timings {
     int64_t taubin_tiles;    /* 256-row tiles of the staged Taubin half-step (last CSR smoothed) */
     int64_t taubin_spill_tiles; /* of those, tiles too large to stage in shared memory, whose rows
                                    gather their neighbours from global memory */
-    int64_t knn_fallback;    /* plain kNN: queries the block-selection search could not certify
+    int64_t knn_fallback;    /* EGT_KNN_SELECT: queries the block selection could not certify
                                 (equal distances, oversized cells, ...) and the ring search ran */
 } egt_timings;
 
@@ -305,6 +305,8 @@ typedef struct egt_batch_timings {
     int64_t csr_nnz;          /* kept neighbours over all clouds */
     int knn_chunk;            /* queries per work claim (autotuned) */
     int taubin_mode;          /* 0 staged tiles, 1 direct gathers (autotuned) */
+    int fused;                /* 1: egt_batch_run ran the kNN and the EGT filter of every cloud in one
+                                 persistent launch (knn_ms; k <= 95); egt_ms is then the CSR packing */
 } egt_batch_timings;
 /* count clouds concatenated in xyz_host ([offsets[count]][3] AoS float),
  * cloud c = points [offsets[c], offsets[c+1]) with k[c] neighbours (1..255). */

@@ -51,7 +51,7 @@ void free_handle(egt_handle* h) {
     for (int L = 0; L < kMaxLevels; L++) {
         F(h->lv[L].order); F(h->lv[L].cell_start); F(h->lv[L].cell_x); F(h->lv[L].row_range);
     }
-    F(h->lists); F(h->kth); F(h->qlevel); F(h->knn_fb); F(h->pclass); F(h->csr_off); F(h->csr_col); F(h->tris); F(h->nrm);
+    F(h->lists); F(h->kth); F(h->qlevel); F(h->pclass); F(h->csr_off); F(h->csr_col); F(h->tris); F(h->nrm);
     F(h->d_counters); F(h->scratch.ptr);
     if (h->taubin_exec) cudaGraphExecDestroy(h->taubin_exec);
     F(h->m_perm); F(h->m_inv); F(h->m_p); F(h->m_pb); F(h->m_off); F(h->m_col);
@@ -126,8 +126,8 @@ egt_status create_common(const float* xyz, bool xyz_on_device, int64_t n, const 
         return EGT_ERR_ARG;
     }
     if (cfg.max_points_in_cell < 1) { set_error("max_points_in_cell must be >= 1"); return EGT_ERR_ARG; }
-    if (cfg.knn_mode != EGT_KNN_PLAIN && cfg.knn_mode != EGT_KNN_LEARNED && cfg.knn_mode != EGT_KNN_RING) {
-        set_error("knn_mode must be EGT_KNN_PLAIN, EGT_KNN_LEARNED or EGT_KNN_RING");
+    if (cfg.knn_mode != EGT_KNN_PLAIN && cfg.knn_mode != EGT_KNN_LEARNED && cfg.knn_mode != EGT_KNN_SELECT) {
+        set_error("knn_mode must be EGT_KNN_PLAIN, EGT_KNN_LEARNED or EGT_KNN_SELECT");
         return EGT_ERR_ARG;
     }
     EGT_CUDA_TRY(cudaSetDevice(cfg.device));

@@ -34,6 +34,7 @@
 #include "grid_common.cuh"
 #include "knn_common.cuh"
 #include "knn_search.cuh"
+#include "knn_select.cuh"
 
 using egt::KnnArgs;
 using egt::LevelDev;
@@ -277,6 +278,7 @@ __global__ void k_make_desc(DescArgs d, KnnArgs* __restrict__ out) {
     a.kth_out = d.kth + o;
     a.qlevel = d.qlevel + o;
     a.counters = d.ctr + (size_t)c * kCtrWords;
+    a.gbase = o;
     out[c] = a;
 }
 
@@ -322,6 +324,56 @@ __global__ void __launch_bounds__(kWarps * 32) k_knn_batch(const KnnArgs* __rest
         }
     }
 }
+
+// kNN and EGT filter of every cloud in one persistent launch: a warp claims
+// one chunk of queries of some cloud per atomic, runs the reference's ring
+// search for each query (as k_knn_batch does), then filters the query's list
+// with the EGT test (egt_query, one query per warp) and stores its kept count
+// for the CSR.  S: list registers for k+1 slots; Se: filter slots per lane.
+template <int S, int Se>
+__global__ void __launch_bounds__(kWarps * 32, 3) k_knn_egt_batch(const KnnArgs* __restrict__ desc,
+                                                                  const int64_t* __restrict__ chunkoff, int count,
+                                                                  unsigned long long* __restrict__ work, float alpha,
+                                                                  int* __restrict__ counts) {
+    __shared__ SelScratch s_sc[kWarps];  // ring-search scratch, then the filter's staged positions
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    SelScratch& sc = s_sc[w];
+    const int64_t total = chunkoff[count];
+    for (;;) {
+        unsigned long long g = 0;
+        if (lane == 0) g = atomicAdd(work, 1ull);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        if ((int64_t)g >= total) break;
+        int lo = 0, hi = count - 1;  // cloud of chunk g
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (chunkoff[mid] <= (int64_t)g) lo = mid;
+            else hi = mid - 1;
+        }
+        const KnnArgs& a = desc[lo];
+        const NormParams np = *a.np;
+        const int q0 = (int)(((int64_t)g - chunkoff[lo]) * a.chunk);
+        const int q1 = min(q0 + a.chunk, a.n);
+        for (int q = q0; q < q1; q++) {
+            const float4 pq = a.p4[q];
+            WarpList<S> L;
+            bool invalid, rerun;
+            const int reached = plain_query<true, S>(a, np, q, pq, L, invalid, lane, sc.pref, sc.start, sc.cd, sc.cj,
+                                                     rerun);
+            write_query<S>(a, q, L, invalid, reached, lane);
+            if (rerun && lane == 0) atomicAdd(&a.counters[kCtrExactRerun], 1ull);
+            __syncwarp();  // the row is written; the scratch is reused
+            unsigned tests = 0;  // not reported for batches
+            const int cnt = egt_query<Se, 32>(a.p4, pq, a.lists + (size_t)q * a.k, a.k, alpha, lane, tests,
+                                              reinterpret_cast<float4*>(sc.d));
+            if (lane == 0) counts[a.gbase + q] = cnt;
+            __syncwarp();
+        }
+    }
+}
+
+// Largest k the fused launch takes (k+1 list slots in three registers per lane).
+constexpr int kFusedMaxK = 95;
 
 // One query per group of G lanes (32 / G queries per warp, possibly of
 // different clouds: each group filters with its own cloud's k).
@@ -454,6 +506,34 @@ egt_status run_knn_batch_s(egt_batch* b, cudaStream_t st) {
     return EGT_OK;
 }
 
+// Blocks of one resident wave of a kernel, per (kernel, device).
+template <typename K>
+egt_status kernel_wave(K kernel, int device, unsigned* out) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), device);
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+        int sms = 0, per = 0;
+        EGT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        EGT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kWarps * 32, 0));
+        it = cache.emplace(key, std::max(1, sms * std::max(per, 1))).first;
+    }
+    *out = (unsigned)it->second;
+    return EGT_OK;
+}
+
+template <int S, int Se>
+egt_status run_knn_egt_batch_s(egt_batch* b, float alpha, int* counts, cudaStream_t st) {
+    unsigned G = 0;
+    EGT_TRY(kernel_wave(k_knn_egt_batch<S, Se>, b->cfg.device, &G));
+    k_knn_egt_batch<S, Se><<<G, kWarps * 32, 0, st>>>(b->d_desc, b->d_chunkoff, b->count,
+                                                      b->h->d_counters + kCtrWork, alpha, counts);
+    EGT_LAUNCH_CHECK();
+    return EGT_OK;
+}
+
 // (Re)builds the chunk prefix and the descriptors' chunk for `chunk`.
 egt_status set_chunk(egt_batch* b, int chunk) {
     if (b->chunkoff_for == chunk) return EGT_OK;
@@ -537,6 +617,36 @@ egt_status filter_batch(egt_batch* b, float alpha) {
     if (s == EGT_OK) s = csr_batch(b, counts);
     EGT_CUDA_TRY(cudaEventRecord(b->h->ev[5], st));
     cudaFreeAsync(counts, st);
+    return s;
+}
+
+// kNN and EGT filter of every cloud in one persistent launch (the lists end
+// filtered), then the CSR of the kept neighbours.  knn_ms times the fused
+// launch, egt_ms the CSR packing.
+egt_status knn_egt_batch(egt_batch* b, float alpha) {
+    cudaStream_t st = b->h->stream;
+    const int64_t N = b->N;
+    EGT_TRY(set_chunk(b, b->chunk > 0 ? b->chunk : kChunk));
+    EGT_CUDA_TRY(cudaMemsetAsync(b->h->d_counters + kCtrWork, 0, sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaMemset2DAsync(b->d_ctr + kCtrInvalid, sizeof(unsigned long long) * kCtrWords, 0,
+                                   2 * sizeof(unsigned long long), b->count, st));
+    EGT_CUDA_TRY(cudaMemset2DAsync(b->d_ctr + kCtrExactRerun, sizeof(unsigned long long) * kCtrWords, 0,
+                                   sizeof(unsigned long long), b->count, st));
+    int* counts = nullptr;
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&counts, sizeof(int) * (N + 1), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(counts + N, 0, sizeof(int), st));
+    EGT_CUDA_TRY(cudaEventRecord(b->h->ev[2], st));
+    const int kk = b->kmax;
+    egt_status s = kk + 1 <= 32   ? run_knn_egt_batch_s<1, 1>(b, alpha, counts, st)
+                   : kk + 1 <= 64 ? run_knn_egt_batch_s<2, 2>(b, alpha, counts, st)
+                                  : run_knn_egt_batch_s<3, 3>(b, alpha, counts, st);
+    if (s == EGT_OK) s = cudaEventRecord(b->h->ev[3], st) == cudaSuccess ? EGT_OK : EGT_ERR_CUDA;
+    if (s == EGT_OK) s = cudaEventRecord(b->h->ev[4], st) == cudaSuccess ? EGT_OK : EGT_ERR_CUDA;
+    b->have_knn = true;
+    if (s == EGT_OK) s = csr_batch(b, counts);
+    if (s == EGT_OK) s = cudaEventRecord(b->h->ev[5], st) == cudaSuccess ? EGT_OK : EGT_ERR_CUDA;
+    cudaFreeAsync(counts, st);
+    b->tm.fused = s == EGT_OK ? 1 : 0;
     return s;
 }
 
@@ -876,8 +986,13 @@ egt_status egt_batch_run(egt_batch* b, int iters, float lambda, float mu, float 
     // every run smooths the input clouds, whatever earlier calls did
     EGT_CUDA_TRY(cudaMemcpyAsync(b->h->p4, b->p4_input, sizeof(float4) * b->N, cudaMemcpyDeviceToDevice, b->h->stream));
     EGT_TRY(autotune(b, lambda, mu, alpha));
-    EGT_TRY(knn_batch(b));
-    EGT_TRY(filter_batch(b, alpha));
+    if (b->kmax <= kFusedMaxK) {
+        EGT_TRY(knn_egt_batch(b, alpha));
+    } else {
+        b->tm.fused = 0;
+        EGT_TRY(knn_batch(b));
+        EGT_TRY(filter_batch(b, alpha));
+    }
     return taubin_batch(b, iters, lambda, mu);
 }
 

@@ -112,9 +112,7 @@ constexpr int kCtrWork = 43;        // work queue of the persistent kNN kernels 
 constexpr int kCtrEvals = 44;       // plain kNN: candidate distances evaluated (reset with 42)
 constexpr int kCtrEgtTests = 45;    // EGT filter: ellipsoid tests of the last filter run
 constexpr int kCtrSpillTiles = 46;  // Taubin tiles that gather from global memory (too large to stage)
-constexpr int kCtrSelWork = 47;     // work queue of the selection kNN kernel
-constexpr int kCtrSelFallback = 48; // queries the selection kNN handed to the ring search (their count)
-constexpr int kCtrFbWork = 49;      // work queue of the ring search over those queries
+constexpr int kCtrSelFallback = 48; // queries the selection kNN could not certify (the ring search ran them)
 
 // One level of the cell hierarchy.  Cells are sorted by key
 // x + y*B + z*B^2; a row is the set of occupied cells sharing (y, z).
@@ -156,7 +154,6 @@ struct egt_handle {
     int* lists = nullptr;        // [n*k] sorted-space lists
     float* kth = nullptr;        // [n] k-th distance per query (diagnostics / learned labels)
     uint8_t* qlevel = nullptr;   // [n] level at which each query stopped
-    int* knn_fb = nullptr;       // [n] queries the selection kNN left to the ring search
     // learned search proposal
     uint8_t* pclass = nullptr;   // [n] proposed class per query
     bool maxpop_valid = false;   // counters[kCtrMaxPop..] match the current grid

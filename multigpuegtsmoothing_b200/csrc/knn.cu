@@ -76,34 +76,45 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_plain(KnnArgs a
     if (threadIdx.x == 0 && s_rerun) atomicAdd(&a.counters[kCtrExactRerun], (unsigned long long)s_rerun);
 }
 
-// Block-selection search (knn_select.cuh), persistent like k_knn_plain.
-// Queries it cannot certify are appended to fb (count *nfb) for the ring
-// search.
-__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_select(KnnArgs a, int* __restrict__ fb,
-                                                                         unsigned long long* __restrict__ nfb) {
+// Block-selection search (knn_select.cuh), persistent like k_knn_plain.  A
+// query it cannot certify runs the ring search right away in the same warp
+// (plain_query; S = list registers per lane for k+1 slots), so the rare slow
+// queries overlap with the rest of the launch.
+template <int S>
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_select(KnnArgs a) {
     __shared__ SelScratch s_sc[kWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    SelScratch& sc = s_sc[w];
     const NormParams np = *a.np;
     // every distance admitted (the under-full rule then always continues)
     const bool usable = np.thres > 4.0f;
     const int n = launch_size(a);
-    unsigned evals = 0;
+    unsigned evals = 0, ring = 0, reruns = 0;
     int gstart = 0, maxlevel = 0;
     for (int q0 = claim(a, lane, n); q0 < n; q0 = claim(a, lane, n)) {
         const int q1 = min(q0 + a.chunk, n);
         for (int jq = q0; jq < q1; jq++) {
             const int q = a.qmap ? a.qmap[jq] : jq;
+            const float4 pq = a.p4[q];
             SelOut r{false, 0, 0.0f};
-            if (usable) r = sel_query(a, np, q, a.p4[q], lane, s_sc[w], gstart, evals);
-            if (lane == 0) {
-                if (r.ok) {
+            if (usable) r = sel_query(a, np, q, pq, lane, sc, gstart, evals);
+            if (r.ok) {
+                if (lane == 0) {
                     if (a.kth_out) a.kth_out[q] = r.kth;
                     if (a.qlevel) a.qlevel[q] = (uint8_t)r.reached;
                     maxlevel = max(maxlevel, r.reached);
-                } else {
-                    fb[atomicAdd(nfb, 1ull)] = q;
                 }
+                continue;
             }
+            WarpList<S> L;
+            bool invalid, rerun;
+            const int reached = plain_query<true, S>(a, np, q, pq, L, invalid, lane, sc.pref, sc.start, sc.cd, sc.cj,
+                                                     rerun);
+            write_query<S>(a, q, L, invalid, reached, lane);
+            __syncwarp();  // the scratch is rewritten by the next query
+            evals += L.ev;
+            ++ring;
+            reruns += rerun ? 1u : 0u;
         }
     }
 #pragma unroll
@@ -111,6 +122,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_knn_select(KnnArgs 
     if (lane == 0) {
         if (evals) atomicAdd(&a.counters[kCtrEvals], (unsigned long long)evals);
         if (maxlevel) atomicMax(&a.counters[kCtrMaxLevel], (unsigned long long)maxlevel);
+        if (ring) atomicAdd(a.n_ring ? a.n_ring : &a.counters[kCtrSelFallback], (unsigned long long)ring);
+        if (reruns) atomicAdd(&a.counters[kCtrExactRerun], (unsigned long long)reruns);
     }
 }
 
@@ -756,7 +769,6 @@ static egt_status knn_prepare(egt_handle* h, int k, KnnArgs* a) {
     }
     if (!h->kth) EGT_CUDA_TRY(dev_alloc(h, &h->kth, sizeof(float) * n));
     if (!h->qlevel) EGT_CUDA_TRY(dev_alloc(h, &h->qlevel, n));
-    if (!h->knn_fb) EGT_CUDA_TRY(dev_alloc(h, &h->knn_fb, sizeof(int) * n));
     h->have_csr = false;
     a->p4 = h->p4;
     a->np = h->d_norm;
@@ -786,26 +798,16 @@ static egt_status knn_launch(const KnnArgs& a, cudaStream_t st) {
     return EGT_OK;
 }
 
-// Device words of one exact search over a.n queries: the selection kernel's
-// work counter, its list of uncertified queries (room for a.n) and their
-// count, and the ring search's work counter over that list.  All counters
-// must be zero.
-struct SearchSlots {
-    unsigned long long* sel_work;
-    unsigned long long* nfb;
-    unsigned long long* fb_work;
-    int* fb;
-};
-
 template <typename K>
 static egt_status select_blocks(K kernel, unsigned* out) {
     static std::mutex mu;
-    static std::map<int, unsigned> cache;
+    static std::map<std::pair<const void*, int>, unsigned> cache;
     int dev = 0;
     EGT_CUDA_TRY(cudaGetDevice(&dev));
+    const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
     {
         std::lock_guard<std::mutex> lock(mu);
-        auto it = cache.find(dev);
+        auto it = cache.find(key);
         if (it != cache.end()) { *out = it->second; return EGT_OK; }
     }
     int sms = 0, per = 0;
@@ -813,28 +815,36 @@ static egt_status select_blocks(K kernel, unsigned* out) {
     EGT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kWarps * 32, 0));
     *out = (unsigned)std::max(1, sms * std::max(per, 1));
     std::lock_guard<std::mutex> lock(mu);
-    cache[dev] = *out;
+    cache[key] = *out;
     return EGT_OK;
 }
 
-// The exact plain search of a.n queries: the block-selection kernel, then the
-// ring search over the queries it could not certify (lists of more than
-// kSelMaxK neighbours run the ring search alone).
-static egt_status knn_search(const KnnArgs& a, const SearchSlots& sl, bool ring_only, cudaStream_t st) {
-    if (ring_only || a.k > kSelMaxK) return knn_launch(a, st);
-    KnnArgs as = a;
-    as.work = sl.sel_work;
+// Queries a warp of the selection kernel claims at a time: consecutive
+// queries lie in nearby cells and mostly take the same level.
+constexpr int kSelChunk = 16;
+
+template <int S>
+static egt_status launch_select(const KnnArgs& a, cudaStream_t st) {
     unsigned G = 0;
-    EGT_TRY(select_blocks(k_knn_select, &G));
-    const int64_t need = ((int64_t)a.n + kWarps * kChunk - 1) / (kWarps * kChunk);
+    EGT_TRY(select_blocks(k_knn_select<S>, &G));
+    const int64_t need = ((int64_t)a.n + kWarps * a.chunk - 1) / (kWarps * a.chunk);
     G = (unsigned)std::max<int64_t>(1, std::min<int64_t>(G, need));
-    k_knn_select<<<G, kWarps * 32, 0, st>>>(as, sl.fb, sl.nfb);
+    k_knn_select<S><<<G, kWarps * 32, 0, st>>>(a);
     EGT_LAUNCH_CHECK();
-    KnnArgs af = a;
-    af.qmap = sl.fb;
-    af.n_dev = sl.nfb;
-    af.work = sl.fb_work;
-    return knn_launch(af, st);
+    return EGT_OK;
+}
+
+// The exact search of a.n queries (the work counter must be zero): the
+// reference's ring search (k_knn_plain), or with `select` (EGT_KNN_SELECT, k <=
+// kSelMaxK) the block-selection kernel, whose uncertified queries run the ring
+// search in the same launch.
+static egt_status knn_search(const KnnArgs& a, bool select, cudaStream_t st) {
+    if (!select || a.k > kSelMaxK) return knn_launch(a, st);
+    KnnArgs as = a;
+    as.chunk = kSelChunk;
+    if (a.k + 1 <= 32) return launch_select<1>(as, st);
+    if (a.k + 1 <= 64) return launch_select<2>(as, st);
+    return launch_select<3>(as, st);
 }
 
 egt_status run_knn(egt_handle* h, int k) {
@@ -844,11 +854,9 @@ egt_status run_knn(egt_handle* h, int k) {
     EGT_TRY(level_maxpop(h));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, 3 * sizeof(unsigned long long), st));
-    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrSelWork, 0, 3 * sizeof(unsigned long long), st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrSelFallback, 0, sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
-    const SearchSlots sl{h->d_counters + kCtrSelWork, h->d_counters + kCtrSelFallback, h->d_counters + kCtrFbWork,
-                         h->knn_fb};
-    EGT_TRY(knn_search(a, sl, h->cfg.knn_mode == EGT_KNN_RING, st));
+    EGT_TRY(knn_search(a, h->cfg.knn_mode == EGT_KNN_SELECT, st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[3], st));
     return EGT_OK;
 }
@@ -936,9 +944,9 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
     EGT_CUDA_TRY(cudaMallocAsync((void**)&idx, sizeof(int) * n, st));
     EGT_CUDA_TRY(cudaMallocAsync((void**)&qmap, sizeof(int) * n, st));
     EGT_CUDA_TRY(cudaMallocAsync((void**)&out, sizeof(int) * (size_t)n * k, st));
-    // per chunk: ring-search work counter, selection work counter, uncertified count, their ring-search counter
-    EGT_CUDA_TRY(cudaMallocAsync((void**)&work, sizeof(unsigned long long) * 4 * chunks, st));
-    EGT_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long) * 4 * chunks, st));
+    // per chunk: its work counter and its count of queries the ring search ran
+    EGT_CUDA_TRY(cudaMallocAsync((void**)&work, sizeof(unsigned long long) * 2 * chunks, st));
+    EGT_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long) * 2 * chunks, st));
     EGT_TRY(level_maxpop(h));
     const unsigned T = 256;
     k_chunk_keys<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(h->perm, n, cb, key, idx);
@@ -976,9 +984,8 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
         ac.qmap = qmap + r0;
         ac.n = m;
         ac.work = work + c;
-        // the chunk's uncertified queries go to fb[r0, r0 + m)
-        const SearchSlots sl{work + chunks + c, work + 2 * chunks + c, work + 3 * chunks + c, h->knn_fb + r0};
-        s = knn_search(ac, sl, h->cfg.knn_mode == EGT_KNN_RING, cs);
+        ac.n_ring = work + chunks + c;
+        s = knn_search(ac, h->cfg.knn_mode == EGT_KNN_SELECT, cs);
         if (s != EGT_OK) break;
         const int64_t cnt = (int64_t)m * k;
         k_rows_original<<<(unsigned)((cnt + T - 1) / T), T, 0, cs>>>(h->lists, h->perm, qmap + r0, m, k, out);
@@ -995,7 +1002,7 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
     if (s == EGT_OK) fail(cudaEventRecord(ev[2 * chunks + 1], ss[1]), "cudaEventRecord");
     if (s == EGT_OK) fail(cudaStreamWaitEvent(st, ev[2 * chunks + 1], 0), "cudaStreamWaitEvent");
     if (s == EGT_OK) {
-        k_sum_counts<<<1, 32, 0, st>>>(work + 2 * chunks, chunks, h->d_counters + kCtrSelFallback);
+        k_sum_counts<<<1, 32, 0, st>>>(work + chunks, chunks, h->d_counters + kCtrSelFallback);
         count_launch();
         fail(cudaGetLastError(), "k_sum_counts");
     }
@@ -1108,7 +1115,6 @@ egt_status run_knn_learned(egt_handle* h, int k, const egt_proposal* p) {
     }
     if (!h->kth) EGT_CUDA_TRY(dev_alloc(h, &h->kth, sizeof(float) * n));
     if (!h->qlevel) EGT_CUDA_TRY(dev_alloc(h, &h->qlevel, n));
-    if (!h->knn_fb) EGT_CUDA_TRY(dev_alloc(h, &h->knn_fb, sizeof(int) * n));
     h->have_csr = false;
     EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
     EGT_TRY(level_maxpop(h));

@@ -22,6 +22,8 @@ struct KnnArgs {
     const int* __restrict__ qmap = nullptr;  // query j of a launch is qmap[j] (nullptr: j)
     unsigned long long* __restrict__ work = nullptr;  // work counter (nullptr: counters[kCtrWork])
     const unsigned long long* __restrict__ n_dev = nullptr;  // launch size on the device (nullptr: n)
+    unsigned long long* __restrict__ n_ring = nullptr;  // ring-search query count (nullptr: counters[kCtrSelFallback])
+    int64_t gbase = 0;  // index of the cloud's first point in a batch's point arrays
 };
 
 // Queries of a launch: n, or the count a preceding kernel left on the device.

@@ -18,29 +18,31 @@
 //
 // So one warp per query:
 //   1. gathers the 3x3x3 block of level-G cells around the query (G from the
-//      previous query of the warp, lowered when the level below holds plenty
-//      of points) as one flattened candidate sequence, 32 per step;
-//   2. bounds the squared distances that can be trusted to be complete: every
-//      point of the cloud within (face distance - 2e-6) of the query lies in
-//      the block (the margin covers the float rounding of cell keys and
-//      distances), so the points below that bound in the block are all such
-//      points of the cloud;
-//   3. pass 1: computes every candidate distance (the reference's contracted
-//      form), keeps it in shared memory, and counts the distances below the
-//      bound into 64 linear buckets;
-//   4. if fewer than k+1 are below the bound, moves to level G+1; otherwise the
-//      bucket holding the (k+1)-th smallest is found by a warp scan, pass 2
-//      collects the distances of that and lower buckets, and a warp bitonic
-//      sort orders them: these are the cloud's k+1 nearest points;
+//      previous query of the warp, one lower when that block holds 4(k+1)
+//      points) as one flattened candidate sequence, 32 per step;
+//   2. completeness: every point of the cloud within (nearest in-grid block
+//      face - 2e-6) of the query lies in the block (the margin covers the float
+//      rounding of cell keys and distances), so the block's points below that
+//      bound are all such points of the cloud;
+//   3. pass 1 computes every distance (the reference's contracted form), keeps
+//      it in shared memory and counts those below the bound into 64 linear
+//      buckets; fewer than k+1 below the bound: next level; else a warp scan
+//      finds the bucket of the (k+1)-th smallest and pass 2 collects that
+//      bucket and the lower ones;
+//   4. sorts the collected candidates (warp bitonic sort): their k+1 smallest
+//      are the cloud's k+1 nearest points;
 //   5. certifies the result: k+1 distinct distances; the stop step s* of the
 //      reference replayed with its own face test (decide) on T; the k nearest
 //      inside the block of step s* (their cell keys); no oversized cell on the
 //      levels up to s*.  A certified query's row is written.  Any other query
-//      is appended to a list that the ring search (k_knn_plain, the exact
-//      insertion rule included) then runs.
+//      runs the ring search (the exact insertion rule included) in the same
+//      warp.
 // The lists are therefore bit-identical to the ring search's, tie order
-// included, while each candidate costs a distance, a bucket count and a
-// shared-memory store instead of a list merge.
+// included.  A candidate costs a distance, a bucket count and a shared-memory
+// store instead of a list merge, but the whole block is evaluated, about 2.3
+// times the candidates the ring search's per-level culling evaluates on the
+// 4M-point superquadric workload; there the ring search is faster and is
+// egt_knn's default (this path is EGT_KNN_SELECT).
 #pragma once
 #include <climits>
 #include "egt_internal.cuh"
@@ -56,8 +58,9 @@ constexpr int kSelCollect = 128;  // collected candidates per query (the (k+1)-t
 constexpr int kSelCache = 1024;   // candidate distances kept between the two passes
 constexpr int kSelMaxK = 95;      // k + 1 <= 96 leaves room in the collection for the boundary bucket
 
-// Per-warp shared scratch of the selection kernel.
-struct SelScratch {
+// Per-warp shared scratch of the selection kernel (16-byte aligned: a fused
+// filter stages float4 positions in `d`).
+struct alignas(16) SelScratch {
     float d[kSelCache];
     int hist[kSelBuckets];
     float cd[kSelCollect];
@@ -155,7 +158,7 @@ struct SelOut {
 // Sorts the collected candidates, certifies them and, when certified, writes
 // query q's row.  c = collected count (k+1 <= c <= kSelCollect).
 template <int R>
-__device__ __forceinline__ SelOut sel_finish(const KnnArgs& a, const NormParams& np, int q, float4 pq, int G, int lane,
+__device__ __noinline__ SelOut sel_finish(const KnnArgs& a, const NormParams& np, int q, float4 pq, int G, int lane,
                                              const SelScratch& sc, int c, const RangeSeq& seq) {
     SelOut out{false, 0, 0.0f};
     const int k = a.k;

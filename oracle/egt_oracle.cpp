@@ -1114,6 +1114,36 @@ void orc_normals(const float* pos, int n, int k, const int* lists, int use_f64, 
     }
 }
 
+// Relative gap (l1 - l0) / l2 of the two smallest eigenvalues of each point's
+// FP64 covariance (the one normal_of<double> solves): where it is ~0 the normal
+// is not defined (any direction in the plane of the two is one).
+void orc_normal_gaps(const float* pos, int n, int k, const int* lists, double* gap) {
+    const float* X = pos;
+    const float* Y = pos + n;
+    const float* Z = pos + 2 * (size_t)n;
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int i = 0; i < n; i++) {
+        const int* row = lists + (size_t)i * k;
+        double sx = X[i], sy = Y[i], sz = Z[i];
+        int cnt = 1;
+        for (int j = 0; j < k; j++) {
+            const int m = row[j];
+            if (m >= 0) { sx += X[m]; sy += Y[m]; sz += Z[m]; cnt++; }
+        }
+        const double cx = sx / cnt, cy = sy / cnt, cz = sz / cnt;
+        double c00 = 0, c01 = 0, c02 = 0, c11 = 0, c12 = 0, c22 = 0;
+        for (int j = 0; j < k; j++) {
+            const int m = row[j];
+            if (m < 0) continue;
+            const double dx = X[m] - cx, dy = Y[m] - cy, dz = Z[m] - cz;
+            c00 += dx * dx; c01 += dx * dy; c02 += dx * dz; c11 += dy * dy; c12 += dy * dz; c22 += dz * dz;
+        }
+        double ev[3], vec[3][3];
+        eigen3<double>(c00, c01, c02, c11, c12, c22, ev, vec);
+        gap[i] = ev[2] > 0 ? (ev[1] - ev[0]) / ev[2] : 0.0;
+    }
+}
+
 // Orientation of GetNormals (Normal_CUDA.cu:329-711) on sorted-space normals,
 // in place.  Undirected edges (min,max) from the lists with weight
 // max(0, 1-|n_u.n_v|) (Normal_CUDA.cu:146-175), deduplicated by the key

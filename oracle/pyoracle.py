@@ -42,6 +42,7 @@ def lib():
         L.orc_taubin_f64.argtypes = [vp, i32, i32, vp, i32, C.c_double, C.c_double]
         L.orc_taubin_rows_f32.argtypes = [vp, i32, i32, vp, vp, f32, vp]
         L.orc_normals.argtypes = [vp, i32, i32, vp, i32, vp]
+        L.orc_normal_gaps.argtypes = [vp, i32, i32, vp, vp]
         L.orc_orient.restype = i32
         L.orc_orient.argtypes = [i32, i32, vp, vp, vp]
         L.orc_orient_kruskal.argtypes = [vp, C.c_int64, i32, i32, vp, vp, vp, i32]
@@ -151,6 +152,17 @@ def normals(pos: np.ndarray, lists: np.ndarray, f64: bool = False) -> np.ndarray
     out = np.empty((3, n), np.float32)
     lib().orc_normals(_p(pos), n, k, _p(lists), int(f64), _p(out))
     return out
+
+
+def normal_gaps(pos: np.ndarray, lists: np.ndarray) -> np.ndarray:
+    """(l1 - l0) / l2 of each point's FP64 covariance (sorted space): ~0 where
+    the normal is not defined."""
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    lists = np.ascontiguousarray(lists, dtype=np.int32)
+    n, k = lists.shape
+    gap = np.empty(n, np.float64)
+    lib().orc_normal_gaps(_p(pos), n, k, _p(lists), _p(gap))
+    return gap
 
 
 def orient(nrm: np.ndarray, lists: np.ndarray):
