@@ -38,6 +38,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_POINTS = 4_000_000
+KNN_MODES = {"plain": 0, "select": 2}  # egt_config.knn_mode: EGT_KNN_PLAIN, EGT_KNN_SELECT
 K = 40
 ITERS = 300
 ALPHA = 0.65
@@ -197,7 +198,7 @@ def fp32_rates(knn_evals, knn_ms, egt_tests, egt_ms, clk):
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_kind": f"nominal FP32 at {mhz:.0f} MHz"}
 
-    return {"knn": one(knn_evals, 8, knn_ms, "candidate distances (k_knn_plain, timed step)"),
+    return {"knn": one(knn_evals, 8, knn_ms, "candidate distances (the kNN kernel, timed step)"),
             "egt": one(egt_tests, 24, egt_ms, "ellipsoid tests (k_egt)")}
 
 
@@ -413,12 +414,15 @@ def batched(capi, iters: int = 150, alpha: float = 0.65):
     b.close()
     n = int(t["points"])
     return {"workload": f"{len(clouds)} clouds, 2K-500K points log-uniform, k in {{10,20,40}}, "
-                        f"EGT + {iters} Taubin iterations, one launch per stage",
+                        f"EGT + {iters} Taubin iterations (kNN + EGT in one fused launch or two, autotuned)",
             "points": n, "grid_ms": t["grid_ms"], "knn_ms": t["knn_ms"], "egt_ms": t["egt_ms"],
             "taubin_ms": t["taubin_ms"], "total_ms": total, "knn_mqueries_s": n / t["knn_ms"] / 1e3,
             "taubin_point_iters_per_s": n * iters / (t["taubin_ms"] * 1e-3),
             "clouds_bit_identical_to_single": f"{same}/{len(sample)}",
-            "knn_chunk": t["knn_chunk"], "taubin_mode": t["taubin_mode"]}
+            "knn_chunk": t["knn_chunk"], "taubin_mode": t["taubin_mode"],
+            "knn_egt_fused": bool(t["fused"]),
+            "autotune_knn_egt_ms": {"one_fused_launch": t["fused_ms"], "two_launches": t["separate_ms"],
+                                    "note": "kNN + EGT filter + CSR, measured by the autotuner; the faster runs"}}
 
 
 def pipeline_configs(capi):
@@ -464,7 +468,8 @@ def run_b200(args, world, rank, local):
     n = xyz.shape[0]
     xyz_dev = torch.from_numpy(xyz).to(dev).contiguous()
     torch.cuda.synchronize()
-    g = capi.GridStructure(None, device_ptr=xyz_dev.data_ptr(), n=n)
+    g = capi.GridStructure(None, device_ptr=xyz_dev.data_ptr(), n=n,
+                           config=capi.default_config(knn_mode=KNN_MODES[args.knn_mode]))
 
     def step():
         g.UpdatePointsDevice(xyz_dev.data_ptr())
@@ -503,6 +508,7 @@ def run_b200(args, world, rank, local):
     # roofline of the dominant kernel (the kNN query kernel): algorithmic bytes
     # 24 + 4k per query (own point 12 B, amortised grid point 12 B, k ids)
     peak, peak_kind = peaks()
+    knn_kernel = "k_knn_plain" if args.knn_mode == "plain" else "k_knn_select"
     knn_bytes = n * (24 + 4 * K)
     knn_gbs = knn_bytes / (knn_ms * 1e-3) / 1e9
 
@@ -580,7 +586,7 @@ def run_b200(args, world, rank, local):
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": f"superquadrics {n} points, 50:1 clustered density, k=40 exact grid kNN",
-                       "n_points": n, "k": K, "parallelism": f"replicas{world}",
+                       "n_points": n, "k": K, "parallelism": f"replicas{world}", "search": args.knn_mode,
                        "l2": "per-step footprint > L2 (n*k*4 = 640 MB of lists written per step)"},
             "stages_ms": {"grid_build": build_ms, "knn_query": knn_ms, "egt_filter": t_egt,
                           "egt_filter_kernel": t_egt_kernel,
@@ -598,7 +604,7 @@ def run_b200(args, world, rank, local):
                                 "m_mean": mbar, "traffic": profiled_traffic("k_taubin_tiles"),
                                 "kernel": "k_taubin_tiles (one half-step)"},
             "roofline": {"bound": "hbm", "achieved": knn_gbs, "peak": peak, "unit": "GB/s", "frac": knn_gbs / peak,
-                         "traffic": profiled_traffic("k_knn_plain"), "kernel": "k_knn_plain",
+                         "traffic": profiled_traffic(knn_kernel), "kernel": knn_kernel,
                          "peak_kind": peak_kind,
                          "bytes_model": "n*(24+4k)"},
             "e2e": {"value": e2e_value, "unit": "Mqueries/s", "h2d_bytes_per_step": int(xyz.nbytes),
@@ -638,6 +644,8 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal comparison")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-clouds workload")
     ap.add_argument("--no-configs", action="store_true", help="skip the 36K-sphere and torus-mesh stage times")
+    ap.add_argument("--knn-mode", default="plain", choices=sorted(KNN_MODES),
+                    help="search of the timed step: plain (the ring search, egt_knn's default) or select")
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="workload size override (profiling a smaller case of the same step)")
     args = ap.parse_args()

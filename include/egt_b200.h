@@ -306,7 +306,10 @@ typedef struct egt_batch_timings {
     int knn_chunk;            /* queries per work claim (autotuned) */
     int taubin_mode;          /* 0 staged tiles, 1 direct gathers (autotuned) */
     int fused;                /* 1: egt_batch_run ran the kNN and the EGT filter of every cloud in one
-                                 persistent launch (knn_ms; k <= 95); egt_ms is then the CSR packing */
+                                 persistent launch (knn_ms; k <= 95); egt_ms is then the CSR packing.
+                                 The autotuner picks that launch or the two separate ones, whichever
+                                 it measured faster: */
+    float fused_ms, separate_ms; /* the autotuner's measurements (kNN + filter + CSR), 0 if not run */
 } egt_batch_timings;
 /* count clouds concatenated in xyz_host ([offsets[count]][3] AoS float),
  * cloud c = points [offsets[c], offsets[c+1]) with k[c] neighbours (1..255). */

@@ -68,7 +68,8 @@ class BatchTimings(C.Structure):
     _fields_ = [("grid_ms", C.c_float), ("knn_ms", C.c_float), ("egt_ms", C.c_float), ("taubin_ms", C.c_float),
                 ("output_ms", C.c_float), ("tune_ms", C.c_float), ("clouds", C.c_int), ("points", C.c_int64),
                 ("invalid_queries", C.c_int64), ("exact_reruns", C.c_int64), ("csr_nnz", C.c_int64),
-                ("knn_chunk", C.c_int), ("taubin_mode", C.c_int), ("fused", C.c_int)]
+                ("knn_chunk", C.c_int), ("taubin_mode", C.c_int), ("fused", C.c_int), ("fused_ms", C.c_float),
+                ("separate_ms", C.c_float)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -66,6 +66,7 @@ struct egt_batch {
     int chunk = 0;                   // 0 = not tuned yet
     int chunkoff_for = 0;            // chunk size d_chunkoff was built for
     int taubin_mode = 0;
+    int fuse = -1;                   // egt_batch_run: 1 fused kNN+EGT launch, 0 separate (-1: not tuned)
     float4* p4_input = nullptr;      // [N] sorted, normalised input positions (egt_batch_run starts here)
     bool tuning_fixed = false;
     bool have_knn = false, have_csr = false;
@@ -679,7 +680,10 @@ struct TuneKey {
     }
 };
 std::mutex g_tune_mu;
-std::map<TuneKey, std::pair<int, int>> g_tune;
+struct TuneVal {
+    int chunk, taubin_mode, fuse;
+};
+std::map<TuneKey, TuneVal> g_tune;
 
 egt_status autotune(egt_batch* b, float lambda, float mu, float alpha) {
     if (b->tuning_fixed || b->chunk > 0) return EGT_OK;
@@ -688,8 +692,9 @@ egt_status autotune(egt_batch* b, float lambda, float mu, float alpha) {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         auto it = g_tune.find(key);
         if (it != g_tune.end()) {
-            b->chunk = it->second.first;
-            b->taubin_mode = it->second.second;
+            b->chunk = it->second.chunk;
+            b->taubin_mode = it->second.taubin_mode;
+            b->fuse = it->second.fuse;
             return EGT_OK;
         }
     }
@@ -711,8 +716,25 @@ egt_status autotune(egt_batch* b, float lambda, float mu, float alpha) {
         if (ms < best) { best = ms; best_chunk = c; }
     }
     b->chunk = best_chunk;
+    // kNN + filter: one fused launch or two, whichever is faster here
+    b->fuse = 0;
+    bool filtered = false;  // the lists are filtered and the CSR built (by the two-launch run)
+    if (b->kmax <= kFusedMaxK) {
+        EGT_TRY(knn_egt_batch(b, alpha));  // warm
+        EGT_TRY(knn_egt_batch(b, alpha));
+        EGT_CUDA_TRY(cudaEventSynchronize(h->ev[5]));
+        const float fused_ms = elapsed_ms(h->ev[2], h->ev[5]);
+        EGT_TRY(knn_batch(b));
+        EGT_TRY(filter_batch(b, alpha));
+        EGT_CUDA_TRY(cudaEventSynchronize(h->ev[5]));
+        const float sep_ms = elapsed_ms(h->ev[2], h->ev[3]) + elapsed_ms(h->ev[4], h->ev[5]);
+        b->fuse = fused_ms < sep_ms ? 1 : 0;
+        b->tm.fused_ms = fused_ms;
+        b->tm.separate_ms = sep_ms;
+        filtered = true;
+    }
     // Taubin kernel: a few half-steps of each on a copy of the positions
-    EGT_TRY(filter_batch(b, alpha));
+    if (!filtered) EGT_TRY(filter_batch(b, alpha));
     float4* save = nullptr;
     EGT_CUDA_TRY(cudaMallocAsync((void**)&save, sizeof(float4) * b->N, st));
     EGT_CUDA_TRY(cudaMemcpyAsync(save, h->p4, sizeof(float4) * b->N, cudaMemcpyDeviceToDevice, st));
@@ -737,7 +759,7 @@ egt_status autotune(egt_batch* b, float lambda, float mu, float alpha) {
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    g_tune[key] = {b->chunk, b->taubin_mode};
+    g_tune[key] = {b->chunk, b->taubin_mode, b->fuse};
     return EGT_OK;
 }
 
@@ -986,7 +1008,7 @@ egt_status egt_batch_run(egt_batch* b, int iters, float lambda, float mu, float 
     // every run smooths the input clouds, whatever earlier calls did
     EGT_CUDA_TRY(cudaMemcpyAsync(b->h->p4, b->p4_input, sizeof(float4) * b->N, cudaMemcpyDeviceToDevice, b->h->stream));
     EGT_TRY(autotune(b, lambda, mu, alpha));
-    if (b->kmax <= kFusedMaxK) {
+    if (b->kmax <= kFusedMaxK && b->fuse != 0) {
         EGT_TRY(knn_egt_batch(b, alpha));
     } else {
         b->tm.fused = 0;

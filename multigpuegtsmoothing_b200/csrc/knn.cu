@@ -851,12 +851,13 @@ egt_status run_knn(egt_handle* h, int k) {
     cudaStream_t st = h->stream;
     KnnArgs a;
     EGT_TRY(knn_prepare(h, k, &a));
-    EGT_TRY(level_maxpop(h));
+    const bool select = h->cfg.knn_mode == EGT_KNN_SELECT;
+    if (select) EGT_TRY(level_maxpop(h));  // the selection's oversized-cell check
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrInvalid, 0, 2 * sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrExactRerun, 0, 3 * sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrSelFallback, 0, sizeof(unsigned long long), st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[2], st));
-    EGT_TRY(knn_search(a, h->cfg.knn_mode == EGT_KNN_SELECT, st));
+    EGT_TRY(knn_search(a, select, st));
     EGT_CUDA_TRY(cudaEventRecord(h->ev[3], st));
     return EGT_OK;
 }
@@ -947,7 +948,7 @@ egt_status run_knn_host(egt_handle* h, int k, int* host) {
     // per chunk: its work counter and its count of queries the ring search ran
     EGT_CUDA_TRY(cudaMallocAsync((void**)&work, sizeof(unsigned long long) * 2 * chunks, st));
     EGT_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long) * 2 * chunks, st));
-    EGT_TRY(level_maxpop(h));
+    if (h->cfg.knn_mode == EGT_KNN_SELECT) EGT_TRY(level_maxpop(h));
     const unsigned T = 256;
     k_chunk_keys<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(h->perm, n, cb, key, idx);
     EGT_LAUNCH_CHECK();
