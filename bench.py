@@ -320,29 +320,16 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def learned_vs_plain(capi):
-    """The learned-proposal workload: 20M points on Gaussian-thickened planar
-    and spherical sheets with a 1000:1 density range, k=64.  A proposal
-    network is trained on two 2M-point clouds of the same generator
-    (seeds 100, 101) with the device's own training kernels, its class
-    threshold is tuned by timing, and the plain grid kNN and the
-    proposal-driven kNN are each timed (best of 3, CUDA events around the
-    search, the proposal's features and network included) and their lists
-    compared for identity."""
-    from multigpuegtsmoothing_b200 import datagen
-    k = 64
-    cache = os.path.join(tempfile.gettempdir(), "egt_bench_sheets_20000000_5.npy")
-    try:
-        xyz = np.load(cache)
-    except (OSError, ValueError):
-        xyz = datagen.sheets(20_000_000, seed=5)
-        try:
-            np.save(cache, xyz)
-        except OSError:
-            pass
+def learned_compare(capi, xyz, k, train, workload):
+    """Trains a proposal network on the clouds `train` with the device's own
+    training kernels, tunes its class threshold by timing, then times on xyz
+    the plain grid kNN (egt_knn's default ring search), the proposal-driven kNN
+    and the block-selection search (best of 3 each, CUDA events around the
+    search, the proposal's features and network included), and compares their
+    lists for identity."""
     p = capi.SearchProposal(k, seed=1)
-    for seed in (100, 101):
-        gt = capi.GridStructure(datagen.sheets(2_000_000, seed=seed))
+    for pts in train:
+        gt = capi.GridStructure(pts)
         gt.GRIDCUDAKNNSELF_COMPACT(k)
         p.collect(gt)
         gt.close()
@@ -364,7 +351,7 @@ def learned_vs_plain(capi):
     same = bool(np.array_equal(g.sorted_lists(), ref)) and bool(np.array_equal(sel.sorted_lists(), ref))
     sel.close()
     n = xyz.shape[0]
-    out = {"workload": f"sheets {n} points, 1000:1 density range, k={k}",
+    out = {"workload": workload,
            "plain": "egt_knn's default: the reference's ring expansion (k_knn_plain)",
            "plain_ms": min(plain_ms), "learned_ms": min(learned_ms),
            "plain_mqueries_s": n / min(plain_ms) / 1e3, "learned_mqueries_s": n / min(learned_ms) / 1e3,
@@ -376,6 +363,35 @@ def learned_vs_plain(capi):
     g.close()
     p.close()
     return out
+
+
+def learned_vs_plain(capi):
+    """The learned-proposal workload: 20M points on Gaussian-thickened planar
+    and spherical sheets with a 1000:1 density range, k=64, the network trained
+    on two 2M-point clouds of the same generator (seeds 100, 101)."""
+    from multigpuegtsmoothing_b200 import datagen
+    k = 64
+    cache = os.path.join(tempfile.gettempdir(), "egt_bench_sheets_20000000_5.npy")
+    try:
+        xyz = np.load(cache)
+    except (OSError, ValueError):
+        xyz = datagen.sheets(20_000_000, seed=5)
+        try:
+            np.save(cache, xyz)
+        except OSError:
+            pass
+    train = [datagen.sheets(2_000_000, seed=s) for s in (100, 101)]
+    return learned_compare(capi, xyz, k, train, f"sheets {xyz.shape[0]} points, 1000:1 density range, k={k}")
+
+
+def learned_on_headline(capi, xyz):
+    """The same comparison on the headline workload (the 4M-point superquadric
+    cloud, k=40), the network trained on two 2M-point superquadric clouds of
+    other seeds (100, 101)."""
+    from multigpuegtsmoothing_b200 import datagen
+    train = [datagen.superquadrics(2_000_000, seed=s) for s in (100, 101)]
+    return learned_compare(capi, xyz, K, train,
+                           f"superquadrics {xyz.shape[0]} points, 50:1 clustered density, k={K}")
 
 
 def batched(capi, iters: int = 150, alpha: float = 0.65):
@@ -625,6 +641,7 @@ def run_b200(args, world, rank, local):
             line["reference_gpu"] = ref_gpu
         if not args.no_learned:
             line["learned_vs_plain"] = learned_vs_plain(capi)
+            line["learned_vs_plain_headline"] = learned_on_headline(capi, xyz)
         if not args.no_batched:
             line["batched"] = batched(capi)
         if world == 1 and not args.no_cpu_baseline:
