@@ -3,7 +3,8 @@
 Workload (one step): the 4,000,000-point superquadric cloud with a 50:1
 clustered density (multigpuegtsmoothing_b200.datagen.superquadrics, seed 3) --
 normalisation, cell sort and hierarchy build, then the exact k=40 grid kNN
-(the reference's GridStructure + GRIDCUDAKNNSELF_COMPACT semantics).  `value`
+(the reference's GridStructure + GRIDCUDAKNNSELF_COMPACT semantics; the
+cell-tile search, egt_knn's default, unless --knn-mode says otherwise).  `value`
 is queries per second over the whole step with the points already in HBM;
 `e2e` is the same through the C ABI from pinned host memory (H2D of the
 points, provider creation, kNN, D2H of the n*k neighbour ids in original
@@ -38,7 +39,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_POINTS = 4_000_000
-KNN_MODES = {"plain": 0, "select": 2}  # egt_config.knn_mode: EGT_KNN_PLAIN, EGT_KNN_SELECT
+KNN_MODES = {"plain": 0, "select": 2, "tile": 3}  # egt_config.knn_mode: EGT_KNN_PLAIN, _SELECT, _TILE
 K = 40
 ITERS = 300
 ALPHA = 0.65
@@ -198,7 +199,8 @@ def fp32_rates(knn_evals, knn_ms, egt_tests, egt_ms, clk):
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_kind": f"nominal FP32 at {mhz:.0f} MHz"}
 
-    return {"knn": one(knn_evals, 8, knn_ms, "candidate distances (the kNN kernel, timed step)"),
+    return {"knn": one(knn_evals, 8, knn_ms, "candidate (query, point) pairs of the kNN search, timed step "
+                                             "(the cell-tile search computes each pair twice, counted once)"),
             "egt": one(egt_tests, 24, egt_ms, "ellipsoid tests (k_egt)")}
 
 
@@ -334,12 +336,13 @@ def learned_compare(capi, xyz, k, train, workload):
         p.collect(gt)
         gt.close()
     losses = p.train(3000)
-    g = capi.GridStructure(xyz)
+    g = capi.GridStructure(xyz, config=capi.default_config(knn_mode=KNN_MODES["plain"]))
     g.GRIDCUDAKNNSELF_COMPACT(k)
     ref = g.sorted_lists()
     p.tune(g)
-    sel = capi.GridStructure(xyz, config=capi.default_config(knn_mode=2))
-    plain_ms, learned_ms, select_ms = [], [], []
+    sel = capi.GridStructure(xyz, config=capi.default_config(knn_mode=KNN_MODES["select"]))
+    til = capi.GridStructure(xyz, config=capi.default_config(knn_mode=KNN_MODES["tile"]))
+    plain_ms, learned_ms, select_ms, tile_ms = [], [], [], []
     for _ in range(3):
         g.GRIDCUDAKNNSELF_COMPACT(k)
         plain_ms.append(g.timings()["knn_ms"])
@@ -348,18 +351,24 @@ def learned_compare(capi, xyz, k, train, workload):
         t = g.timings()
         sel.GRIDCUDAKNNSELF_COMPACT(k)
         select_ms.append(sel.timings()["knn_ms"])
-    same = bool(np.array_equal(g.sorted_lists(), ref)) and bool(np.array_equal(sel.sorted_lists(), ref))
+        til.GRIDCUDAKNNSELF_COMPACT(k)
+        tile_ms.append(til.timings()["knn_ms"])
+    same = all(bool(np.array_equal(x.sorted_lists(), ref)) for x in (g, sel, til))
     sel.close()
+    til.close()
     n = xyz.shape[0]
     out = {"workload": workload,
-           "plain": "egt_knn's default: the reference's ring expansion (k_knn_plain)",
+           "plain": "EGT_KNN_PLAIN: the reference's ring expansion (k_knn_plain)",
            "plain_ms": min(plain_ms), "learned_ms": min(learned_ms),
            "plain_mqueries_s": n / min(plain_ms) / 1e3, "learned_mqueries_s": n / min(learned_ms) / 1e3,
            "speedup": min(plain_ms) / min(learned_ms), "lists_identical": same, "tau": p.tau,
            "box_queries_frac": t["box_queries"] / n, "certified_frac": t["certified_queries"] / n,
            "train_loss_first_last": [float(losses[0]), float(losses[-1])],
            "block_selection_ms": min(select_ms), "block_selection_mqueries_s": n / min(select_ms) / 1e3,
-           "block_selection_note": "the block-selection search (EGT_KNN_SELECT) on the same cloud, same lists"}
+           "block_selection_note": "the block-selection search (EGT_KNN_SELECT) on the same cloud, same lists",
+           "tile_ms": min(tile_ms), "tile_mqueries_s": n / min(tile_ms) / 1e3,
+           "tile_note": "the cell-tile search (EGT_KNN_TILE, egt_knn's default; the ring search for k outside "
+                        "16..40) on the same cloud, same lists"}
     g.close()
     p.close()
     return out
@@ -524,7 +533,7 @@ def run_b200(args, world, rank, local):
     # roofline of the dominant kernel (the kNN query kernel): algorithmic bytes
     # 24 + 4k per query (own point 12 B, amortised grid point 12 B, k ids)
     peak, peak_kind = peaks()
-    knn_kernel = "k_knn_plain" if args.knn_mode == "plain" else "k_knn_select"
+    knn_kernel = {"plain": "k_knn_plain", "select": "k_knn_select", "tile": "k_knn_tile"}[args.knn_mode]
     knn_bytes = n * (24 + 4 * K)
     knn_gbs = knn_bytes / (knn_ms * 1e-3) / 1e9
 
@@ -630,8 +639,9 @@ def run_b200(args, world, rank, local):
             "clocks": clk,
             "knn_stats": {"invalid_queries": tm["invalid_queries"], "levels_used": tm["levels_used"],
                           "ring_search_queries": tm["knn_fallback"], "exact_reruns": tm["exact_reruns"],
-                          "note": "ring_search_queries: rows the block selection could not certify "
-                                  "(equal distances, ...), searched by the reference's ring expansion"},
+                          "note": "ring_search_queries: rows the cell tiles (or the block selection) did not "
+                                  "take or could not certify (equal distances, a k-th ball beyond the block, "
+                                  "...), searched by the reference's ring expansion"},
             "taubin_tiles": {"tiles": spill["taubin_tiles"], "spilled": spill["taubin_spill_tiles"]},
         }
         if configs is not None:
@@ -661,8 +671,9 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal comparison")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-clouds workload")
     ap.add_argument("--no-configs", action="store_true", help="skip the 36K-sphere and torus-mesh stage times")
-    ap.add_argument("--knn-mode", default="plain", choices=sorted(KNN_MODES),
-                    help="search of the timed step: plain (the ring search, egt_knn's default) or select")
+    ap.add_argument("--knn-mode", default="tile", choices=sorted(KNN_MODES),
+                    help="search of the timed step: tile (the cell-tile search, egt_knn's default), plain (the "
+                         "reference's ring search) or select")
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="workload size override (profiling a smaller case of the same step)")
     args = ap.parse_args()

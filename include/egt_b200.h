@@ -46,6 +46,9 @@ typedef struct egt_proposal egt_proposal;
 #define EGT_KNN_PLAIN 0    /* the reference's ring expansion, one warp per query */
 #define EGT_KNN_LEARNED 1  /* proposal-driven box search, certified rows; the ring search for the rest */
 #define EGT_KNN_SELECT 2   /* block selection, certified rows; the ring search for the rest */
+#define EGT_KNN_TILE 3     /* cell tiles (default): a cell's queries one per lane over its 3x3x3
+                              block, certified rows; the ring search for the rest.  For 16 <= k <= 40;
+                              other k use the ring search */
 
 /* Tunables.  Defaults reproduce the reference CLI (main.cpp:108-116). */
 typedef struct egt_config {
@@ -54,9 +57,9 @@ typedef struct egt_config {
     int bucket_count;        /* level-0 buckets per axis (1024) */
     float threshold;         /* GRIDCUDAKNNSELF_COMPACT thres before scaling (1e8) */
     int max_points_in_cell;  /* MAX_PNTS_IN_CUBE (100000): larger cells invalidate a query */
-    int knn_mode;            /* EGT_KNN_PLAIN (default), EGT_KNN_SELECT, or EGT_KNN_LEARNED: egt_knn
-                                uses the proposal attached with egt_attach_proposal.  All three
-                                give identical lists. */
+    int knn_mode;            /* EGT_KNN_TILE (default), EGT_KNN_PLAIN, EGT_KNN_SELECT, or
+                                EGT_KNN_LEARNED: egt_knn uses the proposal attached with
+                                egt_attach_proposal.  All four give identical lists. */
     int warps_per_block;     /* kNN/EGT launch shape (0 = autotuned default) */
     float normals_gap_tol;   /* FP64 eigensolve when (l1-l0) < tol*l2 (0.1; 0 = FP32 only) */
 } egt_config;
@@ -90,13 +93,15 @@ typedef struct egt_timings {
     int64_t certified_queries; /* learned kNN: box results certified (the rest ran the plain search) */
     int64_t exact_reruns;    /* kNN queries whose kept distances tied and that were searched again
                                 with the reference's one-at-a-time insertion rule */
-    int64_t knn_evaluations; /* plain kNN: candidate distances evaluated (8 FP32 operations each) */
+    int64_t knn_evaluations; /* kNN: candidate distances evaluated (8 FP32 operations each; the cell-tile
+                                search counts each candidate once per query though it computes it twice) */
     int64_t egt_tests;       /* EGT filter: ellipsoid tests evaluated (24 FP32 operations each) */
     int64_t taubin_tiles;    /* 256-row tiles of the staged Taubin half-step (last CSR smoothed) */
     int64_t taubin_spill_tiles; /* of those, tiles too large to stage in shared memory, whose rows
                                    gather their neighbours from global memory */
-    int64_t knn_fallback;    /* EGT_KNN_SELECT: queries the block selection could not certify
-                                (equal distances, oversized cells, ...) and the ring search ran */
+    int64_t knn_fallback;    /* EGT_KNN_SELECT / EGT_KNN_TILE: queries the block selection or the cell
+                                tiles did not certify (equal distances, oversized cells, a k-th ball
+                                beyond the block, ...) or did not take, which the ring search ran */
 } egt_timings;
 
 void egt_default_config(egt_config* cfg);
@@ -158,8 +163,10 @@ egt_status egt_get_knn_host(egt_handle* h, int* knn_host, void* stream);
  * overlapped: the queries are searched in chunks of original rows, and each
  * chunk's rows are copied to knn_host (n*k ints; pinned memory lets the copy
  * overlap) while the next chunk is searched.  The handle's lists are those
- * of egt_knn.  In EGT_KNN_LEARNED mode the search and the copy run one after
- * the other. */
+ * of egt_knn.  The chunks run the ring search in every mode but
+ * EGT_KNN_LEARNED, where the search and the copy run one after the other
+ * (the cell-tile search finishes cell by cell, not in row order, so its copy
+ * could not start early). */
 egt_status egt_knn_host(egt_handle* h, int k, int* knn_host, void* stream);
 
 /* Query-vs-reference kNN against the handle's points:

@@ -113,6 +113,12 @@ constexpr int kCtrEvals = 44;       // plain kNN: candidate distances evaluated 
 constexpr int kCtrEgtTests = 45;    // EGT filter: ellipsoid tests of the last filter run
 constexpr int kCtrSpillTiles = 46;  // Taubin tiles that gather from global memory (too large to stage)
 constexpr int kCtrSelFallback = 48; // queries the selection kNN could not certify (the ring search ran them)
+constexpr int kCtrTileUnits = 49;    // cell-tile kNN: units (level, cell) to search
+constexpr int kCtrTileWork = 50;     // cell-tile kNN: next unit to claim
+constexpr int kCtrTileRingWork = 51; // cell-tile kNN: work counter of the ring search over its leftovers
+constexpr int kCtrTileQ = 52;        // cell-tile kNN: queries compacted by unit
+constexpr int kCtrTileRing2 = 55;    // cell-tile kNN: queries it could not certify (the ring search ran them)
+constexpr int kCtrTileRingWork1 = 56; // cell-tile kNN: next unselected query for the ring search in the tile kernel
 
 // One level of the cell hierarchy.  Cells are sorted by key
 // x + y*B + z*B^2; a row is the set of occupied cells sharing (y, z).
@@ -159,6 +165,8 @@ struct egt_handle {
     bool maxpop_valid = false;   // counters[kCtrMaxPop..] match the current grid
     const egt_proposal* proposal = nullptr;  // attached for knn_mode == EGT_KNN_LEARNED
     bool last_knn_learned = false;
+    void* tile_mem = nullptr;    // cell-tile kNN: query levels, unit bits, units, leftover queries
+    size_t tile_bytes = 0;
     int* csr_off = nullptr;      // [n+1]
     int* csr_col = nullptr;      // [nnz]
     int64_t csr_cap = 0;

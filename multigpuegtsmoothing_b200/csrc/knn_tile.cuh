@@ -1,0 +1,580 @@
+// Cell-tile exact kNN: the queries of one grid cell are searched together,
+// one query per lane, over the cell's 3x3x3 block of candidates, which is
+// staged 16 at a time in shared memory.
+//
+// The reference's ring search (GridKNNCuda.cu:647-743, driven level by level
+// from :2322-2634) visits, for a query of level-L cell C, the points of the
+// 3x3x3 block of level-L cells around C -- the same block for every query of
+// C.  k_knn_plain runs one query per warp and spends ~16 warp instructions
+// per candidate locating, loading and merging it.  Here each half of a warp
+// takes a cell (a unit) and up to 16 of its queries, one per lane; every
+// candidate of the block is loaded once per half-warp and compared by all
+// of its lanes at once:
+//
+//   pass 1  each lane buckets its candidate distances (64 buckets, 8 per
+//           octave of d^2 from (h/4)^2 to (4h)^2, h the level's cell side)
+//           and finds the bucket b* holding its (k+1)-th smallest;
+//   pass 2  each lane keeps the candidates of buckets <= b* (at most
+//           kTileCap) in bucket order (offsets from pass 1's counts), then
+//           insertion-sorts them (only candidates of one bucket are out of
+//           order).
+//
+// The result is accepted only when it provably equals the ring search's list
+// (the conditions of the proposal-driven box search, knn.cu): the k+1
+// smallest distances are pairwise distinct; the ball of the k-th distance
+// (plus a margin) lies inside the searched block, so the k kept points are
+// the k nearest of the cloud; the ring search's stop step, replayed with
+// decide() on that distance, visits them all; and no cell of the levels it
+// visits holds max_points_in_cell points or more.  Queries whose blocks never
+// reach the population that selects a level run the ring search (k_knn_plain's
+// code) at the start of the same kernel; queries that fail the checks run it
+// afterwards (k_knn_plain over the list of those queries).
+//
+// The level of a query is the first whose block around the query's cell
+// holds at least kTileAlpha * (k+1) points (k_tile_assign); every cell that
+// has queries at its level becomes one unit of work.
+#pragma once
+#include "knn_search.cuh"
+#include "proposal.cuh"
+
+namespace egt {
+namespace {
+
+constexpr int kTileWarps = 1;    // warps per block (one: blocks pack the SM's shared memory tightly)
+constexpr int kTileBins = 64;    // distance buckets per query: 8 per octave of d^2, (h/4)^2 to (4h)^2
+constexpr int kTileCap = 50;     // candidates kept per query (the buckets up to b*, the query included)
+constexpr int kTileMinK = 16;    // smaller k: the ring search (measured faster there)
+constexpr int kTileMaxK = 40;    // largest k the cell-tile search takes
+constexpr int kTileAlpha = 5;    // block population that selects a level, in units of k+1 (measured:
+                                 // 4 to 5.5 within noise on 4M superquadrics at k = 40)
+constexpr int kTileMaxBlock = 6144;   // larger blocks: the ring search (one warp would hold the search's end)
+constexpr int kTileClasses = 6;       // batch classes by block size (>= 4096, 2048, 1024, 512, 256, less)
+
+struct TileArgs {
+    uint8_t* lq;                      // [n] level each query is searched at (0xff: ring search)
+    uint32_t* unit_bits;              // [kMaxLevels][words] cells that already have a unit
+    int words;                        // words per level
+    uint32_t* units;                  // [n] level << 29 | cell index
+    unsigned long long* n_units;      // units written by k_tile_assign
+    unsigned long long* unit_work;    // next unit to claim
+    int* ring;                        // [n] queries for the ring search
+    unsigned long long* n_ring;       // their count
+    int thr;                          // kTileAlpha * (k+1)
+    int maxblock;                     // kTileMaxBlock
+    uint32_t* qarr;                   // [n] the units' queries, grouped by unit (k_tile_gather)
+    unsigned long long* n_q;          // queries written to qarr
+    uint2* batch;                     // [bcap] (unit, first query in qarr), largest blocks first
+    uint8_t* bcnt;                    // [bcap] queries in each batch (1..16)
+    int bcap;                         // n + n/16 + 1 >= units + queries/16
+    uint32_t* ucnt;                   // [n] queries of each unit
+    uint8_t* ucls;                    // [n] class of each unit's block
+    unsigned long long* cls_n;        // [kTileClasses] batches per class
+    unsigned long long* cls_fill;     // [kTileClasses] batches written per class
+    int* ring2;                       // [n] queries the tile search could not certify
+    unsigned long long* n_ring2;      // their count
+    unsigned long long* ring_work;    // next query of `ring` for the tile kernel's ring search
+};
+
+// Shared memory of one warp (both halves).
+constexpr size_t kTileWarpBytes = (size_t)kTileBins * 32 * 4   // bucket counts, then offsets [bucket][lane]
+                                  + (size_t)kTileCap * 32 * 8  // kept candidates, (d bits << 32 | point)
+                                  + 2 * 16 * 16                // staged candidates per half (x, y, z, point)
+                                  + 2 * 2 * 16 * 4;            // range sequence scratch per half
+constexpr size_t kTileSmem = kTileWarpBytes * kTileWarps;
+
+// Kept-candidate slot s of lane `lane`: XOR-swizzled so that the lanes'
+// appends (different slots) spread over the banks.
+__device__ __forceinline__ int tile_slot(int s, int lane) { return s * 32 + (lane ^ (s & 31)); }
+
+// Index of level cell (cx, cy, cz) in the level's cell arrays (-1: empty).
+__device__ __forceinline__ int cell_index(const LevelDev& L, int cx, int cy, int cz) {
+    if (cx < 0 || cx >= L.B || cy < 0 || cy >= L.B || cz < 0 || cz >= L.B) return -1;
+    const int2 rr = L.row_range[cy + cz * L.B];
+    int lo = rr.x, hi = rr.y;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (L.cell_x[mid] < cx) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < rr.y && L.cell_x[lo] == cx) ? lo : -1;
+}
+
+// Appends the flagged values of the warp to a device list (one atomic per warp).
+__device__ __forceinline__ void warp_append(bool flag, uint32_t v, uint32_t* list, unsigned long long* count,
+                                            int lane) {
+    const unsigned m = __ballot_sync(0xffffffffu, flag);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (flag) list[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
+// Level and unit of every query; queries that no level selects (or every
+// query when the admission threshold can cut lists) go to the ring search.
+__global__ void __launch_bounds__(256) k_tile_assign(KnnArgs a, TileArgs t) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool in = q < a.n;
+    int lsel = -1, ci = -1;
+    // thres > 4 exceeds every squared distance of the unit cube: all admitted
+    if (in && a.np->thres > 4.0f) {
+        const uint32_t c0 = __float_as_uint(a.p4[q].w);
+        const int cx0 = c0 & 1023u, cy0 = (c0 >> 10) & 1023u, cz0 = (c0 >> 20) & 1023u;
+        for (int l = 0; l < kMaxLevels && lsel < 0; l++) {
+            const LevelDev& LV = a.lv[l];
+            const int cx = cx0 >> l, cy = cy0 >> l, cz = cz0 >> l;
+            int pop = 0;
+#pragma unroll
+            for (int r = 0; r < 9; r++) {
+                const int2 g = row_points(LV, cx - 1, cx + 1, cy + r % 3 - 1, cz + r / 3 - 1);
+                pop += g.y - g.x;
+            }
+            if (pop >= t.thr) {
+                lsel = pop <= t.maxblock ? l : kMaxLevels;  // kMaxLevels: too large, ring search
+                if (lsel == l) ci = cell_index(LV, cx, cy, cz);
+            }
+        }
+    }
+    if (lsel >= kMaxLevels || ci < 0) lsel = -1;  // ci < 0 cannot happen: the query's own cell is occupied
+    warp_append(in && lsel < 0, (uint32_t)q, reinterpret_cast<uint32_t*>(t.ring), t.n_ring, lane);
+    if (in) t.lq[q] = lsel < 0 ? (uint8_t)0xff : (uint8_t)lsel;
+    bool fresh = false;
+    if (lsel >= 0) {
+        const uint32_t bit = 1u << (ci & 31);
+        fresh = !(atomicOr(t.unit_bits + (size_t)lsel * t.words + (ci >> 5), bit) & bit);
+    }
+    warp_append(fresh, ((uint32_t)lsel << 29) | (uint32_t)ci, t.units, t.n_units, lane);
+}
+
+// Class of a block of `pop` candidates: larger blocks are searched first, and
+// batches claimed together have blocks of similar size (the two halves of a
+// warp run in step, each as long as the larger of their blocks).
+__device__ __forceinline__ int tile_class(int pop) {
+    return pop >= 4096 ? 0 : pop >= 2048 ? 1 : pop >= 1024 ? 2 : pop >= 512 ? 3 : pop >= 256 ? 4 : 5;
+}
+
+// Per unit (one warp per unit, grid-stride): its query count and block class,
+// and the batch count of each class.
+__global__ void __launch_bounds__(256) k_tile_count(KnnArgs a, TileArgs t) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const unsigned long long nu = *t.n_units;
+    for (unsigned long long u = gw; u < nu; u += nw) {
+        const uint32_t code = t.units[u];
+        const int l = (int)(code >> 29), ci = (int)(code & 0x1fffffffu);
+        const LevelDev& LV = a.lv[l];
+        const int* order = l ? LV.order : nullptr;
+        const int cs = LV.cell_start[ci], ce = LV.cell_start[ci + 1];
+        int cnt = 0;
+        for (int s = cs; s < ce; s += 32) {
+            bool sel = false;
+            if (s + lane < ce) {
+                const int qq = order ? order[s + lane] : s + lane;
+                sel = t.lq[qq] == (uint8_t)l;
+            }
+            cnt += __popc(__ballot_sync(0xffffffffu, sel));
+        }
+        const int p0 = order ? order[cs] : cs;
+        const uint32_t cc = __float_as_uint(a.p4[p0].w);
+        const int cx = (int)(cc & 1023u) >> l, cy = (int)((cc >> 10) & 1023u) >> l, cz = (int)((cc >> 20) & 1023u) >> l;
+        int pop = 0;
+        if (lane < 9) {
+            const int2 g = row_points(LV, cx - 1, cx + 1, cy + lane % 3 - 1, cz + lane / 3 - 1);
+            pop = g.y - g.x;
+        }
+        pop = __reduce_add_sync(0xffffffffu, pop);
+        const int cls = tile_class(pop);
+        if (lane == 0) {
+            t.ucnt[u] = (uint32_t)cnt;
+            t.ucls[u] = (uint8_t)cls;
+            atomicAdd(&t.cls_n[cls], (unsigned long long)((cnt + 15) >> 4));
+        }
+    }
+}
+
+// Compacts each unit's queries into qarr and cuts them into batches of up to
+// 16 (one warp per unit, grid-stride), the batches ordered by class.
+__global__ void __launch_bounds__(256) k_tile_gather(KnnArgs a, TileArgs t) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const unsigned long long nu = *t.n_units;
+    // first batch of each class
+    unsigned long long coff = 0;
+    {
+        unsigned long long v = lane < kTileClasses ? t.cls_n[lane] : 0ull;
+        unsigned long long incl = v;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            const unsigned long long w = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += w;
+        }
+        coff = incl - v;
+    }
+    for (unsigned long long u = gw; u < nu; u += nw) {
+        const uint32_t code = t.units[u];
+        const int l = (int)(code >> 29), ci = (int)(code & 0x1fffffffu);
+        const LevelDev& LV = a.lv[l];
+        const int* order = l ? LV.order : nullptr;
+        const int cs = LV.cell_start[ci], ce = LV.cell_start[ci + 1];
+        const int cnt = (int)t.ucnt[u], cls = (int)t.ucls[u];
+        const int nbat = (cnt + 15) >> 4;
+        const unsigned long long base = __shfl_sync(0xffffffffu, coff, cls);
+        unsigned long long qb = 0, bb = 0;
+        if (lane == 0 && cnt > 0) {
+            qb = atomicAdd(t.n_q, (unsigned long long)cnt);
+            bb = base + atomicAdd(&t.cls_fill[cls], (unsigned long long)nbat);
+        }
+        qb = __shfl_sync(0xffffffffu, qb, 0);
+        bb = __shfl_sync(0xffffffffu, bb, 0);
+        int w = 0;
+        for (int s = cs; s < ce && w < cnt; s += 32) {
+            bool sel = false;
+            int qq = -1;
+            if (s + lane < ce) {
+                qq = order ? order[s + lane] : s + lane;
+                sel = t.lq[qq] == (uint8_t)l;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, sel);
+            if (sel) t.qarr[qb + w + __popc(m & ((1u << lane) - 1u))] = (uint32_t)qq;
+            w += __popc(m);
+        }
+        for (int j = lane; j < nbat; j += 32) {
+            t.batch[bb + j] = make_uint2(code, (uint32_t)(qb + 16 * j));
+            t.bcnt[bb + j] = (uint8_t)min(16, cnt - 16 * j);
+        }
+    }
+}
+
+// Half-warp form of range_seq (knn_search.cuh): the ranges of a half's lanes
+// (hl = lane within the half, hf = which half) as one flattened sequence.
+// All 32 lanes call it; each half gets its own sequence.
+__device__ __forceinline__ RangeSeq range_seq16(int sz, int cs, int hl, int hf, int* s_pref, int* s_start) {
+    int incl = sz;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o, 16);
+        if (hl >= o) incl += v;
+    }
+    const unsigned ne = (__ballot_sync(0xffffffffu, sz > 0) >> (16 * hf)) & 0xffffu;
+    RangeSeq q;
+    q.total = __shfl_sync(0xffffffffu, incl, 15, 16);
+    q.m = __popc(ne);
+    __syncwarp();
+    if (sz > 0) {
+        const int r = __popc(ne & ((1u << hl) - 1u));
+        s_pref[r] = incl;
+        s_start[r] = cs;
+    }
+    __syncwarp();
+    q.incl = hl < q.m ? s_pref[hl] : INT_MAX;
+    q.cs = hl < q.m ? s_start[hl] : 0;
+    __syncwarp();
+    return q;
+}
+
+// Half-warp form of seq_index: point index of candidate base + hl of the
+// half's sequence (-1 past its end).  All 32 lanes call it.
+__device__ __forceinline__ int seq_index16(const RangeSeq& q, int base, int hl, int hf,
+                                           const int* __restrict__ order) {
+    const int before = __popc((__ballot_sync(0xffffffffu, q.incl <= base) >> (16 * hf)) & 0xffffu);
+    const int at = q.incl - base;
+    const unsigned sb = (at > 0 && at < 16) ? (1u << at) : 0u;
+    const unsigned starts = (__reduce_or_sync(0xffffffffu, sb << (16 * hf)) >> (16 * hf)) & 0xffffu;
+    const int c = before + __popc(starts & ((2u << hl) - 1u));
+    const int prev_end = __shfl_sync(0xffffffffu, q.incl, (c - 1) & 15, 16);
+    const int cs = __shfl_sync(0xffffffffu, q.cs, c & 15, 16);
+    const int j = base + hl;
+    if (j >= q.total) return -1;
+    const int pos = cs + (j - (c > 0 ? prev_end : 0));
+    return order ? __ldg(order + pos) : pos;
+}
+
+__device__ __forceinline__ uint32_t tile_bin(float d, uint32_t lo) {
+    return min((max(__float_as_uint(d), lo) - lo) >> 20, (uint32_t)(kTileBins - 1));
+}
+
+// State of one half-warp's current unit (uniform within the half).
+struct TileUnit {
+    RangeSeq seq;
+    const int* order;
+    uint32_t lo;   // float bits of the lower edge of bucket 1 less one bucket
+    int l;         // level; -1 = no unit
+};
+
+// Streams both halves' blocks through their staging buffers, 16 candidates
+// per half at a time (the next 16 are loaded while the current ones are
+// compared), calling f(j) for the half's staged candidates j = 0..15 (padding
+// past a block's end lies far away with index -1).
+template <typename F>
+__device__ __forceinline__ void tile_stream16(const TileUnit& U, bool live, int steps, const float4* __restrict__ p4,
+                                              float4* chunk, int hl, int hf, F&& f) {
+    const float4 far = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+    // software pipeline: the point index of step s+2 and the position of
+    // step s+1 are in flight while step s is compared
+    int pB = seq_index16(U.seq, 0, hl, hf, U.order);
+    int pA = seq_index16(U.seq, 16, hl, hf, U.order);
+    if (!live) pA = pB = -1;
+    float4 vB = pB >= 0 ? __ldg(p4 + pB) : far;
+    for (int s = 0; s < steps; s++) {
+        __syncwarp();
+        chunk[hl] = make_float4(vB.x, vB.y, vB.z, __int_as_float(pB));
+        __syncwarp();
+        pB = pA;
+        vB = pB >= 0 ? __ldg(p4 + pB) : far;
+        pA = seq_index16(U.seq, (s + 2) * 16, hl, hf, U.order);
+        if (!live) pA = -1;
+        f();
+    }
+    __syncwarp();
+}
+
+// Sets up a new unit for the lanes with `take` (both halves call it; a half
+// with take = false keeps its unit).
+__device__ __forceinline__ void tile_unit_setup(const KnnArgs& a, const NormParams& np, uint32_t code, bool take,
+                                                int hl, int hf, int* s_pref, int* s_start, TileUnit& U) {
+    const int l = (int)(code >> 29), ci = (int)(code & 0x1fffffffu);
+    int2 rg = make_int2(0, 0);
+    int cx = 0, cy = 0, cz = 0;
+    const int* order = nullptr;
+    if (take) {
+        const LevelDev& LV = a.lv[l];
+        order = l ? LV.order : nullptr;
+        const int cs = LV.cell_start[ci];
+        const int p0 = order ? order[cs] : cs;
+        const uint32_t cc = __float_as_uint(a.p4[p0].w);
+        cx = (int)(cc & 1023u) >> l;
+        cy = (int)((cc >> 10) & 1023u) >> l;
+        cz = (int)((cc >> 20) & 1023u) >> l;
+        if (hl < 9) rg = row_points(LV, cx - 1, cx + 1, cy + hl % 3 - 1, cz + hl / 3 - 1);
+    }
+    const RangeSeq seq = range_seq16(rg.y - rg.x, rg.x, hl, hf, s_pref, s_start);
+    if (take) {
+        U.seq = seq;
+        U.order = order;
+        U.l = l;
+        // buckets: 8 per octave of d^2, bucket 0 below (h/4)^2 and 1/8 octave,
+        // bucket kTileBins-1 from 16 h^2 up
+        const float h = __fmul_rn(__fsub_rn(np.b, np.a), (float)(1 << l) * (1.0f / 1024.0f));
+        U.lo = __float_as_uint(__fmul_rn(16.0f, __fmul_rn(h, h))) - ((uint32_t)(kTileBins - 1) << 20);
+    }
+}
+
+// Persistent: each half-warp claims batches (up to 16 queries of one unit)
+// one at a time; both halves run their batches together.
+__global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArgs t) {
+    extern __shared__ __align__(16) unsigned char s_tile[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int hl = lane & 15, hf = lane >> 4;
+    unsigned char* base = s_tile + (size_t)w * kTileWarpBytes;
+    uint32_t* hist = reinterpret_cast<uint32_t*>(base);
+    unsigned long long* buf = reinterpret_cast<unsigned long long*>(base + (size_t)kTileBins * 32 * 4);
+    float4* chunk = reinterpret_cast<float4*>(buf + (size_t)kTileCap * 32) + 16 * hf;
+    int* s_pref = reinterpret_cast<int*>(reinterpret_cast<float4*>(buf + (size_t)kTileCap * 32) + 32) + 32 * hf;
+    int* s_start = s_pref + 16;
+    uint32_t* hcol = hist + lane;
+    const NormParams np = *a.np;
+    const int k = a.k;
+    unsigned long long evals = 0;
+    unsigned maxlev = 0;
+    // First the ring search (k_knn_plain's code, one query per warp) of the
+    // queries no level selected, while the other warps already search
+    // batches, so that the long ones do not end the search.  Its scratch lies
+    // in the kept-candidate space.  (Queries that fail the checks run it in a
+    // separate launch at the ring kernel's own occupancy: measured faster than
+    // running them here, between batches.)
+    int* r_pref = reinterpret_cast<int*>(buf);
+    int* r_start = r_pref + 32;
+    float* r_md = reinterpret_cast<float*>(r_start + 32);
+    int* r_mp = reinterpret_cast<int*>(r_md + 64);
+    unsigned reruns = 0;
+    auto ring_query = [&](int q) {
+        WarpList<2> L;
+        bool invalid, rerun;
+        const int reached = plain_query<true, 2>(a, np, q, a.p4[q], L, invalid, lane, r_pref, r_start, r_md, r_mp,
+                                                 rerun);
+        write_query<2>(a, q, L, invalid, reached, lane);
+        reruns += rerun ? 1u : 0u;
+        evals += L.ev;
+    };
+    {
+        const unsigned long long n_r = *t.n_ring;
+        for (;;) {
+            unsigned long long j = 0;
+            if (lane == 0) j = atomicAdd(t.ring_work, 1ull);
+            j = __shfl_sync(0xffffffffu, j, 0);
+            if (j >= n_r) break;
+            ring_query(t.ring[j]);
+        }
+        __syncwarp();
+    }
+    for (int b = 0; b < kTileBins; b++) hcol[b * 32] = 0u;
+    const float4* __restrict__ p4 = a.p4;
+    TileUnit U;
+    U.seq.incl = INT_MAX;
+    U.seq.cs = 0;
+    U.seq.m = 0;
+    U.seq.total = 0;
+    U.order = nullptr;
+    U.lo = 0u;
+    U.l = -1;
+    unsigned long long n_batches = 0;
+#pragma unroll
+    for (int c = 0; c < kTileClasses; c++) n_batches += t.cls_n[c];
+    for (;;) {
+        // each half claims one batch: largest blocks first
+        unsigned long long c = 0;
+        if (hl == 0) c = atomicAdd(t.unit_work, 1ull);
+        c = __shfl_sync(0xffffffffu, c, 16 * hf);
+        const bool take = c < n_batches;
+        if (!__any_sync(0xffffffffu, take)) break;
+        const long long bi = take ? (long long)c : 0;
+        const uint2 bd = take ? t.batch[bi] : make_uint2(0u, 0u);
+        const int nq = take ? (int)t.bcnt[bi] : 0;
+        tile_unit_setup(a, np, bd.x, take, hl, hf, s_pref, s_start, U);
+        const bool act = hl < nq;
+        const int q = act ? (int)t.qarr[bd.y + hl] : -1;
+        const float4 pq = act ? p4[q] : make_float4(3e18f, 3e18f, 3e18f, 0.f);
+        const int total = take ? U.seq.total : 0;
+        const int steps = (max(total, __shfl_xor_sync(0xffffffffu, total, 16)) + 15) >> 4;
+        const uint32_t lo = U.lo;
+        // pass 1: bucket counts (the query itself included, at distance 0)
+        tile_stream16(U, take, steps, p4, chunk, hl, hf, [&]() {
+            uint32_t bk[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                const float4 c = chunk[j];
+                bk[j] = tile_bin(fs_dist3(pq.x, pq.y, pq.z, c.x, c.y, c.z), lo);
+            }
+#pragma unroll
+            for (int j = 0; j < 16; j++) atomicAdd(hcol + bk[j] * 32, 1u);
+        });
+        // bucket offsets and the bucket b* of the (k+1)-th distance other
+        // than the query's own
+        int cum = 0, bstar = -1, m = 0;
+#pragma unroll 8
+        for (int b = 0; b < kTileBins; b++) {
+            const int c = (int)hcol[b * 32];
+            hcol[b * 32] = (uint32_t)cum;
+            cum += c;
+            if (bstar < 0 && cum >= k + 2) { bstar = b; m = cum; }
+        }
+        bool ok = act && bstar >= 0 && bstar < kTileBins - 1 && m <= kTileCap;
+        const float T = ok ? __uint_as_float(lo + ((uint32_t)(bstar + 1) << 20)) : 0.0f;
+        // pass 2: the candidates of buckets <= b*, in bucket order
+        tile_stream16(U, take, steps, p4, chunk, hl, hf, [&]() {
+#pragma unroll
+            for (int j0 = 0; j0 < 16; j0 += 8) {
+                float dd[8];
+                int pp[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const float4 c = chunk[j0 + j];
+                    dd[j] = fs_dist3(pq.x, pq.y, pq.z, c.x, c.y, c.z);
+                    pp[j] = __float_as_int(c.w);
+                }
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    if (dd[j] < T) {
+                        const uint32_t s = atomicAdd(hcol + tile_bin(dd[j], lo) * 32, 1u);
+                        reinterpret_cast<uint2*>(buf)[tile_slot((int)s, lane)] =
+                            make_uint2((uint32_t)pp[j], __float_as_uint(dd[j]));
+                    }
+                }
+            }
+        });
+#pragma unroll 8
+        for (int b = 0; b < kTileBins; b++) hcol[b * 32] = 0u;
+        float kth = 0.0f;
+        int reached = 0;
+        int self = 0;  // slot of the query itself after sorting; entry i of the list is slot i + (i >= self)
+        if (ok) {
+            // only candidates of one bucket can be out of order
+            for (int i = 1; i < m; i++) {
+                const unsigned long long e = buf[tile_slot(i, lane)];
+                int j = i;
+                while (j > 0) {
+                    const unsigned long long g = buf[tile_slot(j - 1, lane)];
+                    if (g < e) break;
+                    buf[tile_slot(j, lane)] = g;
+                    j--;
+                }
+                buf[tile_slot(j, lane)] = e;
+            }
+            // the query sits among the distance-0 entries at the front
+            while (self < m - 1 && (uint32_t)buf[tile_slot(self, lane)] != (uint32_t)q) self++;
+            // (1) the k+1 smallest distances pairwise distinct
+            uint32_t prev = (uint32_t)(buf[tile_slot(self == 0 ? 1 : 0, lane)] >> 32);
+            for (int i = 1; i <= k && ok; i++) {
+                const uint32_t cur = (uint32_t)(buf[tile_slot(i + (i >= self), lane)] >> 32);
+                ok = cur != prev;
+                prev = cur;
+            }
+        }
+        if (ok) {
+            const int l = U.l;
+            kth = __uint_as_float((uint32_t)(buf[tile_slot(k - 1 + (k - 1 >= self), lane)] >> 32));
+            const uint32_t c0 = __float_as_uint(pq.w);
+            const int cq[3] = {(int)(c0 & 1023u), (int)((c0 >> 10) & 1023u), (int)((c0 >> 20) & 1023u)};
+            // (2) the k-th ball inside the searched block
+            int lo3[3], end3[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                lo3[d] = ((cq[d] >> l) - 1) << l;
+                end3[d] = ((cq[d] >> l) + 2) << l;
+            }
+            ok = ball_in_box(np, pq, kth, lo3, end3);
+            // (3) the ring search's stop step
+            int sf = -1;
+            if (ok) {
+                for (int st = 0; st <= kMaxLevels; st++) {
+                    const int Ls = st == 0 ? 0 : st - 1, o = st == 0 ? 0 : 1;
+                    if (!decide(np, Ls, o, k, k, kth, false, pq, cq[0], cq[1], cq[2])) { sf = st; break; }
+                }
+                ok = sf >= 0;
+            }
+            if (ok) {
+                const int Lf = sf == 0 ? 0 : sf - 1, of = sf == 0 ? 0 : 1;
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    lo3[d] = ((cq[d] >> Lf) - of) << Lf;
+                    end3[d] = ((cq[d] >> Lf) + of + 1) << Lf;
+                }
+                if (!ball_in_box(np, pq, kth, lo3, end3)) {
+                    for (int i = 0; i < k && ok; i++) {
+                        const int p = (int)(uint32_t)buf[tile_slot(i + (i >= self), lane)];
+                        ok = visit_step(__float_as_uint(p4[p].w), c0) <= sf;
+                    }
+                }
+            }
+            // (4) no oversized cell on the visited levels
+            if (ok)
+                for (int L = 0; L <= max(sf - 1, 0) && ok; L++)
+                    ok = a.counters[kCtrMaxPop + L] < (unsigned long long)a.max_pts;
+            reached = max(sf - 1, 0);
+        }
+        if (ok) {
+            int* row = a.lists + (size_t)q * k;
+            for (int i = 0; i < k; i++) row[i] = (int)(uint32_t)buf[tile_slot(i + (i >= self), lane)];
+            if (a.kth_out) a.kth_out[q] = kth;
+            if (a.qlevel) a.qlevel[q] = (uint8_t)reached;
+            maxlev = max(maxlev, (unsigned)reached);
+        }
+        if (hl == 0) evals += (unsigned long long)total * nq;
+        warp_append(act && !ok, (uint32_t)q, reinterpret_cast<uint32_t*>(t.ring2), t.n_ring2, lane);
+    }
+    maxlev = __reduce_max_sync(0xffffffffu, maxlev);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
+    if (lane == 0) {
+        if (reruns) atomicAdd(&a.counters[kCtrExactRerun], (unsigned long long)reruns);
+        if (evals) atomicAdd(&a.counters[kCtrEvals], evals);
+        if (maxlev) atomicMax(&a.counters[kCtrMaxLevel], (unsigned long long)maxlev);
+    }
+}
+
+}  // namespace
+}  // namespace egt

@@ -20,6 +20,7 @@ def test_version_and_default_config():
     c = capi.default_config()
     assert c.bucket_count == 1024 and abs(c.eps - 1e-6) < 1e-12
     assert c.max_points_in_cell == 100000 and c.threshold == 1e8
+    assert c.knn_mode == 3  # EGT_KNN_TILE
 
 
 def test_null_arguments_rejected_without_gpu():

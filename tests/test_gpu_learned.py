@@ -116,7 +116,8 @@ def test_learned_lists_bit_identical(capi, trained, case, k):
 
 def test_learned_beats_plain(capi, trained):
     p, _ = trained
-    g = capi.GridStructure(datagen.superquadrics(2_000_000, seed=3))
+    # against the ring search (EGT_KNN_PLAIN), the search the proposal replaces
+    g = capi.GridStructure(datagen.superquadrics(2_000_000, seed=3), config=capi.default_config(knn_mode=0))
     g.GRIDCUDAKNNSELF_COMPACT(40)
     p.tune(g)  # the class threshold, chosen by timing as a user would
     best = {"plain": 1e30, "learned": 1e30}
@@ -140,7 +141,7 @@ def test_learned_target_on_sheets(capi):
     planar and spherical sheets with a 1000:1 density range, k = 64, the network
     trained on two 2M-point clouds of the same generator (other seeds) with the
     device's own training kernels.  Target: at least 1.5x the plain grid kNN
-    (the ring search) on the same GPU, lists bit-identical."""
+    (the ring search, EGT_KNN_PLAIN) on the same GPU, lists bit-identical."""
     import os
     import tempfile
     cache = os.path.join(tempfile.gettempdir(), "egt_bench_sheets_20000000_5.npy")
@@ -156,7 +157,7 @@ def test_learned_target_on_sheets(capi):
         p.collect(gt)
         gt.close()
     p.train(3000)
-    g = capi.GridStructure(xyz)
+    g = capi.GridStructure(xyz, config=capi.default_config(knn_mode=0))
     g.GRIDCUDAKNNSELF_COMPACT(k)
     plain = g.sorted_lists()
     p.tune(g)

@@ -126,13 +126,13 @@ def _cloud_case(case):
 @pytest.mark.parametrize("case,k", [("sphere", 40), ("superquadrics", 40), ("superquadrics", 64), ("clusters", 20),
                                     ("clusters", 95), ("dups", 5), ("lattice", 8), ("sphere", 1), ("sphere", 96)])
 def test_select_matches_ring_search(capi, case, k):
-    """The block-selection search (EGT_KNN_SELECT) against egt_knn's default,
-    the reference's ring expansion run query by query: identical lists, invalid
+    """The block-selection search (EGT_KNN_SELECT) against the reference's ring
+    expansion run query by query (EGT_KNN_PLAIN): identical lists, invalid
     rows and deepest level.  Certified rows come from the selection kernel, the
     rest (ties, oversized cells, k > 95) from the ring search in the same warp."""
     xyz = _cloud_case(case)
     g = cloud(capi, xyz, k, capi.default_config(knn_mode=2))
-    r = cloud(capi, xyz, k)
+    r = cloud(capi, xyz, k, capi.default_config(knn_mode=0))
     assert np.array_equal(g.sorted_lists(), r.sorted_lists())
     t, tr = g.timings(), r.timings()
     assert t["invalid_queries"] == tr["invalid_queries"]
@@ -146,6 +146,59 @@ def test_select_matches_ring_search(capi, case, k):
         assert t["knn_fallback"] < 0.05 * n, t["knn_fallback"]
     # the lists in original order through the chunked host path too
     assert np.array_equal(g.knn_host(k), r.GetKNNIndexes())
+    g.close()
+    r.close()
+
+
+@pytest.mark.parametrize("case,k", [("sphere", 40), ("sphere", 16), ("superquadrics", 40), ("superquadrics", 24),
+                                    ("clusters", 20), ("clusters", 40), ("dups", 20), ("lattice", 26),
+                                    ("sphere", 10), ("superquadrics", 41)])
+def test_tile_matches_ring_search(capi, case, k):
+    """The cell-tile search (EGT_KNN_TILE, egt_knn's default for 16 <= k <= 40)
+    against the reference's ring expansion run query by query (EGT_KNN_PLAIN):
+    identical lists, invalid rows and deepest level.  Certified rows come from
+    the tile kernel, the rest (equal distances, a k-th ball beyond the block,
+    blocks too large or too sparse) from the ring search; k outside [16, 40]
+    runs the ring search alone."""
+    xyz = _cloud_case(case)
+    g = cloud(capi, xyz, k)  # the default configuration
+    assert capi.default_config().knn_mode == 3
+    r = cloud(capi, xyz, k, capi.default_config(knn_mode=0))
+    assert np.array_equal(g.sorted_lists(), r.sorted_lists())
+    t, tr = g.timings(), r.timings()
+    assert t["invalid_queries"] == tr["invalid_queries"]
+    assert t["levels_used"] == tr["levels_used"]
+    n = xyz.shape[0]
+    if not 16 <= k <= 40:
+        assert t["knn_fallback"] == 0 and t["knn_evaluations"] == tr["knn_evaluations"]
+    elif case in ("sphere", "superquadrics"):
+        assert t["knn_fallback"] < 0.15 * n, t["knn_fallback"]
+    elif case == "clusters":
+        # the densest cluster's level-0 blocks exceed the tile cap: ring search
+        assert t["knn_fallback"] < 0.5 * n, t["knn_fallback"]
+    elif case == "lattice":
+        assert t["knn_fallback"] == n  # every row has equal distances
+    g.close()
+    r.close()
+
+
+@pytest.mark.parametrize("thres,max_pts", [(0.05, 100000), (1e8, 60)])
+def test_tile_threshold_and_cell_cap(capi, thres, max_pts):
+    """A finite admission threshold sends every query to the ring search; a
+    small max_points_in_cell invalidates rows the same way in both searches."""
+    xyz = _cloud_case("clusters")
+    cfg_t = capi.default_config(max_points_in_cell=max_pts)
+    cfg_r = capi.default_config(knn_mode=0, max_points_in_cell=max_pts)
+    g, r = capi.GridStructure(xyz, config=cfg_t), capi.GridStructure(xyz, config=cfg_r)
+    g.GRIDCUDAKNNSELF_COMPACT(20, thres=thres)
+    r.GRIDCUDAKNNSELF_COMPACT(20, thres=thres)
+    assert np.array_equal(g.sorted_lists(), r.sorted_lists())
+    t, tr = g.timings(), r.timings()
+    assert t["invalid_queries"] == tr["invalid_queries"]
+    if thres < 1.0:
+        assert t["knn_fallback"] == xyz.shape[0]
+    else:
+        assert tr["invalid_queries"] > 0
     g.close()
     r.close()
 
