@@ -14,10 +14,10 @@
 //   pass 1  each lane buckets its candidate distances (64 buckets, 8 per
 //           octave of d^2 from (h/4)^2 to (4h)^2, h the level's cell side)
 //           and finds the bucket b* holding its (k+1)-th smallest;
-//   pass 2  each lane keeps the candidates of buckets <= b* (at most
-//           kTileCap) in bucket order (offsets from pass 1's counts), then
-//           insertion-sorts them (only candidates of one bucket are out of
-//           order).
+//   pass 2  each lane keeps the points of buckets <= b* (at most kTileCap)
+//           in bucket order (offsets from pass 1's counts); their distances
+//           are computed again into the spent bucket space and the list is
+//           insertion-sorted (only candidates of one bucket are out of order).
 //
 // The result is accepted only when it provably equals the ring search's list
 // (the conditions of the proposal-driven box search, knn.cu): the k+1
@@ -42,7 +42,7 @@ namespace {
 
 constexpr int kTileWarps = 1;    // warps per block (one: blocks pack the SM's shared memory tightly)
 constexpr int kTileBins = 64;    // distance buckets per query: 8 per octave of d^2, (h/4)^2 to (4h)^2
-constexpr int kTileCap = 50;     // candidates kept per query (the buckets up to b*, the query included)
+constexpr int kTileCap = 64;     // candidates kept per query (the buckets up to b*, the query included)
 constexpr int kTileMinK = 16;    // smaller k: the ring search (measured faster there)
 constexpr int kTileMaxK = 40;    // largest k the cell-tile search takes
 constexpr int kTileAlpha = 5;    // block population that selects a level, in units of k+1 (measured:
@@ -77,7 +77,7 @@ struct TileArgs {
 
 // Shared memory of one warp (both halves).
 constexpr size_t kTileWarpBytes = (size_t)kTileBins * 32 * 4   // bucket counts, then offsets [bucket][lane]
-                                  + (size_t)kTileCap * 32 * 8  // kept candidates, (d bits << 32 | point)
+                                  + (size_t)kTileCap * 32 * 4  // kept candidates' points [slot][lane], swizzled
                                   + 2 * 16 * 16                // staged candidates per half (x, y, z, point)
                                   + 2 * 2 * 16 * 4;            // range sequence scratch per half
 constexpr size_t kTileSmem = kTileWarpBytes * kTileWarps;
@@ -371,9 +371,9 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
     const int hl = lane & 15, hf = lane >> 4;
     unsigned char* base = s_tile + (size_t)w * kTileWarpBytes;
     uint32_t* hist = reinterpret_cast<uint32_t*>(base);
-    unsigned long long* buf = reinterpret_cast<unsigned long long*>(base + (size_t)kTileBins * 32 * 4);
-    float4* chunk = reinterpret_cast<float4*>(buf + (size_t)kTileCap * 32) + 16 * hf;
-    int* s_pref = reinterpret_cast<int*>(reinterpret_cast<float4*>(buf + (size_t)kTileCap * 32) + 32) + 32 * hf;
+    uint32_t* bidx = reinterpret_cast<uint32_t*>(base + (size_t)kTileBins * 32 * 4);
+    float4* chunk = reinterpret_cast<float4*>(bidx + (size_t)kTileCap * 32) + 16 * hf;
+    int* s_pref = reinterpret_cast<int*>(reinterpret_cast<float4*>(bidx + (size_t)kTileCap * 32) + 32) + 32 * hf;
     int* s_start = s_pref + 16;
     uint32_t* hcol = hist + lane;
     const NormParams np = *a.np;
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
     // in the kept-candidate space.  (Queries that fail the checks run it in a
     // separate launch at the ring kernel's own occupancy: measured faster than
     // running them here, between batches.)
-    int* r_pref = reinterpret_cast<int*>(buf);
+    int* r_pref = reinterpret_cast<int*>(bidx);
     int* r_start = r_pref + 32;
     float* r_md = reinterpret_cast<float*>(r_start + 32);
     int* r_mp = reinterpret_cast<int*>(r_md + 64);
@@ -480,43 +480,48 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
                 for (int j = 0; j < 8; j++) {
                     if (dd[j] < T) {
                         const uint32_t s = atomicAdd(hcol + tile_bin(dd[j], lo) * 32, 1u);
-                        reinterpret_cast<uint2*>(buf)[tile_slot((int)s, lane)] =
-                            make_uint2((uint32_t)pp[j], __float_as_uint(dd[j]));
+                        bidx[tile_slot((int)s, lane)] = (uint32_t)pp[j];
                     }
                 }
             }
         });
-#pragma unroll 8
-        for (int b = 0; b < kTileBins; b++) hcol[b * 32] = 0u;
         float kth = 0.0f;
         int reached = 0;
         int self = 0;  // slot of the query itself after sorting; entry i of the list is slot i + (i >= self)
         if (ok) {
-            // only candidates of one bucket can be out of order
+            // the kept candidates' distances, into the bucket space (its offsets are spent)
+#pragma unroll 4
+            for (int i = 0; i < m; i++) {
+                const float4 v = __ldg(p4 + bidx[tile_slot(i, lane)]);
+                hcol[i * 32] = __float_as_uint(fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z));
+            }
+            // sorted by (distance, point); only candidates of one bucket are out of order
             for (int i = 1; i < m; i++) {
-                const unsigned long long e = buf[tile_slot(i, lane)];
+                const uint32_t ed = hcol[i * 32], ei = bidx[tile_slot(i, lane)];
                 int j = i;
                 while (j > 0) {
-                    const unsigned long long g = buf[tile_slot(j - 1, lane)];
-                    if (g < e) break;
-                    buf[tile_slot(j, lane)] = g;
+                    const uint32_t gd = hcol[(j - 1) * 32], gi = bidx[tile_slot(j - 1, lane)];
+                    if (gd < ed || (gd == ed && gi < ei)) break;
+                    hcol[j * 32] = gd;
+                    bidx[tile_slot(j, lane)] = gi;
                     j--;
                 }
-                buf[tile_slot(j, lane)] = e;
+                hcol[j * 32] = ed;
+                bidx[tile_slot(j, lane)] = ei;
             }
             // the query sits among the distance-0 entries at the front
-            while (self < m - 1 && (uint32_t)buf[tile_slot(self, lane)] != (uint32_t)q) self++;
+            while (self < m - 1 && bidx[tile_slot(self, lane)] != (uint32_t)q) self++;
             // (1) the k+1 smallest distances pairwise distinct
-            uint32_t prev = (uint32_t)(buf[tile_slot(self == 0 ? 1 : 0, lane)] >> 32);
+            uint32_t prev = hcol[(self == 0 ? 1 : 0) * 32];
             for (int i = 1; i <= k && ok; i++) {
-                const uint32_t cur = (uint32_t)(buf[tile_slot(i + (i >= self), lane)] >> 32);
+                const uint32_t cur = hcol[(i + (i >= self)) * 32];
                 ok = cur != prev;
                 prev = cur;
             }
         }
         if (ok) {
             const int l = U.l;
-            kth = __uint_as_float((uint32_t)(buf[tile_slot(k - 1 + (k - 1 >= self), lane)] >> 32));
+            kth = __uint_as_float(hcol[(k - 1 + (k - 1 >= self)) * 32]);
             const uint32_t c0 = __float_as_uint(pq.w);
             const int cq[3] = {(int)(c0 & 1023u), (int)((c0 >> 10) & 1023u), (int)((c0 >> 20) & 1023u)};
             // (2) the k-th ball inside the searched block
@@ -545,7 +550,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
                 }
                 if (!ball_in_box(np, pq, kth, lo3, end3)) {
                     for (int i = 0; i < k && ok; i++) {
-                        const int p = (int)(uint32_t)buf[tile_slot(i + (i >= self), lane)];
+                        const int p = (int)bidx[tile_slot(i + (i >= self), lane)];
                         ok = visit_step(__float_as_uint(p4[p].w), c0) <= sf;
                     }
                 }
@@ -558,13 +563,15 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
         }
         if (ok) {
             int* row = a.lists + (size_t)q * k;
-            for (int i = 0; i < k; i++) row[i] = (int)(uint32_t)buf[tile_slot(i + (i >= self), lane)];
+            for (int i = 0; i < k; i++) row[i] = (int)bidx[tile_slot(i + (i >= self), lane)];
             if (a.kth_out) a.kth_out[q] = kth;
             if (a.qlevel) a.qlevel[q] = (uint8_t)reached;
             maxlev = max(maxlev, (unsigned)reached);
         }
         if (hl == 0) evals += (unsigned long long)total * nq;
         warp_append(act && !ok, (uint32_t)q, reinterpret_cast<uint32_t*>(t.ring2), t.n_ring2, lane);
+#pragma unroll 8
+        for (int b = 0; b < kTileBins; b++) hcol[b * 32] = 0u;
     }
     maxlev = __reduce_max_sync(0xffffffffu, maxlev);
 #pragma unroll
