@@ -14,10 +14,11 @@
 //   pass 1  each lane buckets its candidate distances (64 buckets, 8 per
 //           octave of d^2 from (h/4)^2 to (4h)^2, h the level's cell side)
 //           and finds the bucket b* holding its (k+1)-th smallest;
-//   pass 2  each lane keeps the points of buckets <= b* (at most kTileCap)
-//           in bucket order (offsets from pass 1's counts); their distances
-//           are computed again into the spent bucket space and the list is
-//           insertion-sorted (only candidates of one bucket are out of order).
+//   pass 2  each lane keeps the block positions (16 bits) of buckets <= b*
+//           (at most kTileCap) in bucket order (offsets from pass 1's counts);
+//           their distances are computed again into the spent bucket space
+//           and the list is insertion-sorted (only candidates of one bucket
+//           are out of order).
 //
 // The result is accepted only when it provably equals the ring search's list
 // (the conditions of the proposal-driven box search, knn.cu): the k+1
@@ -77,14 +78,13 @@ struct TileArgs {
 
 // Shared memory of one warp (both halves).
 constexpr size_t kTileWarpBytes = (size_t)kTileBins * 32 * 4   // bucket counts, then offsets [bucket][lane]
-                                  + (size_t)kTileCap * 32 * 4  // kept candidates' points [slot][lane], swizzled
+                                  + (size_t)kTileCap * 32 * 2  // kept candidates' block positions [slot][lane]
                                   + 2 * 16 * 16                // staged candidates per half (x, y, z, point)
                                   + 2 * 2 * 16 * 4;            // range sequence scratch per half
 constexpr size_t kTileSmem = kTileWarpBytes * kTileWarps;
 
-// Kept-candidate slot s of lane `lane`: XOR-swizzled so that the lanes'
-// appends (different slots) spread over the banks.
-__device__ __forceinline__ int tile_slot(int s, int lane) { return s * 32 + (lane ^ (s & 31)); }
+// Kept-candidate slot s of lane `lane` (16-bit entries: two lanes per bank word).
+__device__ __forceinline__ int tile_slot(int s, int lane) { return s * 32 + lane; }
 
 // Index of level cell (cx, cy, cz) in the level's cell arrays (-1: empty).
 __device__ __forceinline__ int cell_index(const LevelDev& L, int cx, int cy, int cz) {
@@ -305,10 +305,21 @@ struct TileUnit {
     int l;         // level; -1 = no unit
 };
 
+// Point index of block position `pos` of a half's unit: the ranges of the
+// unit's block (their inclusive prefix ends and starts, as range_seq16 left
+// them in the half's scratch) are searched for the one holding it.
+__device__ __forceinline__ int tile_point(int pos, const TileUnit& U, const int* s_pref, const int* s_start) {
+    int r = 0;
+#pragma unroll
+    for (int t = 0; t < 9; t++) r += (t < U.seq.m && s_pref[t] <= pos) ? 1 : 0;
+    const int local = s_start[r] + (pos - (r > 0 ? s_pref[r - 1] : 0));
+    return U.order ? __ldg(U.order + local) : local;
+}
+
 // Streams both halves' blocks through their staging buffers, 16 candidates
-// per half at a time (the next 16 are loaded while the current ones are
-// compared), calling f(j) for the half's staged candidates j = 0..15 (padding
-// past a block's end lies far away with index -1).
+// per half at a time, calling f(s) for step s: the half's staged candidates
+// are the block positions 16 s .. 16 s + 15 (padding past a block's end lies
+// far away with index -1).
 template <typename F>
 __device__ __forceinline__ void tile_stream16(const TileUnit& U, bool live, int steps, const float4* __restrict__ p4,
                                               float4* chunk, int hl, int hf, F&& f) {
@@ -327,7 +338,7 @@ __device__ __forceinline__ void tile_stream16(const TileUnit& U, bool live, int 
         vB = pB >= 0 ? __ldg(p4 + pB) : far;
         pA = seq_index16(U.seq, (s + 2) * 16, hl, hf, U.order);
         if (!live) pA = -1;
-        f();
+        f(s);
     }
     __syncwarp();
 }
@@ -371,9 +382,9 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
     const int hl = lane & 15, hf = lane >> 4;
     unsigned char* base = s_tile + (size_t)w * kTileWarpBytes;
     uint32_t* hist = reinterpret_cast<uint32_t*>(base);
-    uint32_t* bidx = reinterpret_cast<uint32_t*>(base + (size_t)kTileBins * 32 * 4);
-    float4* chunk = reinterpret_cast<float4*>(bidx + (size_t)kTileCap * 32) + 16 * hf;
-    int* s_pref = reinterpret_cast<int*>(reinterpret_cast<float4*>(bidx + (size_t)kTileCap * 32) + 32) + 32 * hf;
+    uint16_t* bpos = reinterpret_cast<uint16_t*>(base + (size_t)kTileBins * 32 * 4);
+    float4* chunk = reinterpret_cast<float4*>(bpos + (size_t)kTileCap * 32) + 16 * hf;
+    int* s_pref = reinterpret_cast<int*>(reinterpret_cast<float4*>(bpos + (size_t)kTileCap * 32) + 32) + 32 * hf;
     int* s_start = s_pref + 16;
     uint32_t* hcol = hist + lane;
     const NormParams np = *a.np;
@@ -386,7 +397,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
     // in the kept-candidate space.  (Queries that fail the checks run it in a
     // separate launch at the ring kernel's own occupancy: measured faster than
     // running them here, between batches.)
-    int* r_pref = reinterpret_cast<int*>(bidx);
+    int* r_pref = reinterpret_cast<int*>(bpos);
     int* r_start = r_pref + 32;
     float* r_md = reinterpret_cast<float*>(r_start + 32);
     int* r_mp = reinterpret_cast<int*>(r_md + 64);
@@ -442,7 +453,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
         const int steps = (max(total, __shfl_xor_sync(0xffffffffu, total, 16)) + 15) >> 4;
         const uint32_t lo = U.lo;
         // pass 1: bucket counts (the query itself included, at distance 0)
-        tile_stream16(U, take, steps, p4, chunk, hl, hf, [&]() {
+        tile_stream16(U, take, steps, p4, chunk, hl, hf, [&](int) {
             uint32_t bk[16];
 #pragma unroll
             for (int j = 0; j < 16; j++) {
@@ -465,22 +476,20 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
         bool ok = act && bstar >= 0 && bstar < kTileBins - 1 && m <= kTileCap;
         const float T = ok ? __uint_as_float(lo + ((uint32_t)(bstar + 1) << 20)) : 0.0f;
         // pass 2: the candidates of buckets <= b*, in bucket order
-        tile_stream16(U, take, steps, p4, chunk, hl, hf, [&]() {
+        tile_stream16(U, take, steps, p4, chunk, hl, hf, [&](int st) {
 #pragma unroll
             for (int j0 = 0; j0 < 16; j0 += 8) {
                 float dd[8];
-                int pp[8];
 #pragma unroll
                 for (int j = 0; j < 8; j++) {
                     const float4 c = chunk[j0 + j];
                     dd[j] = fs_dist3(pq.x, pq.y, pq.z, c.x, c.y, c.z);
-                    pp[j] = __float_as_int(c.w);
                 }
 #pragma unroll
                 for (int j = 0; j < 8; j++) {
                     if (dd[j] < T) {
                         const uint32_t s = atomicAdd(hcol + tile_bin(dd[j], lo) * 32, 1u);
-                        bidx[tile_slot((int)s, lane)] = (uint32_t)pp[j];
+                        bpos[tile_slot((int)s, lane)] = (uint16_t)(st * 16 + j0 + j);
                     }
                 }
             }
@@ -492,25 +501,25 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
             // the kept candidates' distances, into the bucket space (its offsets are spent)
 #pragma unroll 4
             for (int i = 0; i < m; i++) {
-                const float4 v = __ldg(p4 + bidx[tile_slot(i, lane)]);
+                const float4 v = __ldg(p4 + tile_point(bpos[tile_slot(i, lane)], U, s_pref, s_start));
                 hcol[i * 32] = __float_as_uint(fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z));
             }
-            // sorted by (distance, point); only candidates of one bucket are out of order
+            // sorted by (distance, block position); only candidates of one bucket are out of order
             for (int i = 1; i < m; i++) {
-                const uint32_t ed = hcol[i * 32], ei = bidx[tile_slot(i, lane)];
+                const uint32_t ed = hcol[i * 32], ei = bpos[tile_slot(i, lane)];
                 int j = i;
                 while (j > 0) {
-                    const uint32_t gd = hcol[(j - 1) * 32], gi = bidx[tile_slot(j - 1, lane)];
+                    const uint32_t gd = hcol[(j - 1) * 32], gi = bpos[tile_slot(j - 1, lane)];
                     if (gd < ed || (gd == ed && gi < ei)) break;
                     hcol[j * 32] = gd;
-                    bidx[tile_slot(j, lane)] = gi;
+                    bpos[tile_slot(j, lane)] = (uint16_t)gi;
                     j--;
                 }
                 hcol[j * 32] = ed;
-                bidx[tile_slot(j, lane)] = ei;
+                bpos[tile_slot(j, lane)] = (uint16_t)ei;
             }
             // the query sits among the distance-0 entries at the front
-            while (self < m - 1 && bidx[tile_slot(self, lane)] != (uint32_t)q) self++;
+            while (self < m - 1 && tile_point(bpos[tile_slot(self, lane)], U, s_pref, s_start) != q) self++;
             // (1) the k+1 smallest distances pairwise distinct
             uint32_t prev = hcol[(self == 0 ? 1 : 0) * 32];
             for (int i = 1; i <= k && ok; i++) {
@@ -550,7 +559,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
                 }
                 if (!ball_in_box(np, pq, kth, lo3, end3)) {
                     for (int i = 0; i < k && ok; i++) {
-                        const int p = (int)bidx[tile_slot(i + (i >= self), lane)];
+                        const int p = tile_point(bpos[tile_slot(i + (i >= self), lane)], U, s_pref, s_start);
                         ok = visit_step(__float_as_uint(p4[p].w), c0) <= sf;
                     }
                 }
@@ -563,7 +572,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
         }
         if (ok) {
             int* row = a.lists + (size_t)q * k;
-            for (int i = 0; i < k; i++) row[i] = (int)bidx[tile_slot(i + (i >= self), lane)];
+            for (int i = 0; i < k; i++) row[i] = tile_point(bpos[tile_slot(i + (i >= self), lane)], U, s_pref, s_start);
             if (a.kth_out) a.kth_out[q] = kth;
             if (a.qlevel) a.qlevel[q] = (uint8_t)reached;
             maxlev = max(maxlev, (unsigned)reached);
