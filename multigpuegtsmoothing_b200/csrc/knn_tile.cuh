@@ -48,6 +48,7 @@ constexpr int kTileMinK = 16;    // smaller k: the ring search (measured faster 
 constexpr int kTileMaxK = 40;    // largest k the cell-tile search takes
 constexpr int kTileAlpha = 5;    // block population that selects a level, in units of k+1 (measured:
                                  // 4 to 5.5 within noise on 4M superquadrics at k = 40)
+constexpr int kTileSparse = 3;       // a finer block below kTileSparse/4 * (k+1) points: the ring search
 constexpr int kTileMaxBlock = 6144;   // larger blocks: the ring search (one warp would hold the search's end)
 constexpr int kTileClasses = 6;       // batch classes by block size (>= 4096, 2048, 1024, 512, 256, less)
 
@@ -62,6 +63,7 @@ struct TileArgs {
     unsigned long long* n_ring;       // their count
     int thr;                          // kTileAlpha * (k+1)
     int maxblock;                     // kTileMaxBlock
+    int sparse;                       // kTileSparse * (k+1) / 4
     uint32_t* qarr;                   // [n] the units' queries, grouped by unit (k_tile_gather)
     unsigned long long* n_q;          // queries written to qarr
     uint2* batch;                     // [bcap] (unit, first query in qarr), largest blocks first
@@ -122,6 +124,7 @@ __global__ void __launch_bounds__(256) k_tile_assign(KnnArgs a, TileArgs t) {
     if (in && a.np->thres > 4.0f) {
         const uint32_t c0 = __float_as_uint(a.p4[q].w);
         const int cx0 = c0 & 1023u, cy0 = (c0 >> 10) & 1023u, cz0 = (c0 >> 20) & 1023u;
+        int prev = INT_MAX;  // population of the block one level finer
         for (int l = 0; l < kMaxLevels && lsel < 0; l++) {
             const LevelDev& LV = a.lv[l];
             const int cx = cx0 >> l, cy = cy0 >> l, cz = cz0 >> l;
@@ -132,9 +135,13 @@ __global__ void __launch_bounds__(256) k_tile_assign(KnnArgs a, TileArgs t) {
                 pop += g.y - g.x;
             }
             if (pop >= t.thr) {
-                lsel = pop <= t.maxblock ? l : kMaxLevels;  // kMaxLevels: too large, ring search
+                // kMaxLevels: a block too large, or a query alone in its finer
+                // block -- the ring search (such a query's k nearest lie far
+                // off, beyond the block, and its search climbs high)
+                lsel = pop <= t.maxblock && prev >= t.sparse ? l : kMaxLevels;
                 if (lsel == l) ci = cell_index(LV, cx, cy, cz);
             }
+            prev = pop;
         }
     }
     if (lsel >= kMaxLevels || ci < 0) lsel = -1;  // ci < 0 cannot happen: the query's own cell is occupied
