@@ -898,7 +898,7 @@ static egt_status tile_prepare(egt_handle* h, int k, TileArgs* t) {
     t->ring_work = h->d_counters + kCtrTileRingWork1;
     t->thr = kTileAlpha * (k + 1);
     t->maxblock = kTileMaxBlock;
-    t->sparse = kTileSparse * (k + 1) / 4;
+    t->sparse = (k + 1) / kTileSparse;
     cudaStream_t st = h->stream;
     EGT_CUDA_TRY(cudaMemsetAsync(t->unit_bits, 0, b_bits, st));
     EGT_CUDA_TRY(cudaMemsetAsync(tctr, 0, b_ctr, st));

@@ -46,9 +46,12 @@ constexpr int kTileBins = 64;    // distance buckets per query: 8 per octave of 
 constexpr int kTileCap = 64;     // candidates kept per query (the buckets up to b*, the query included)
 constexpr int kTileMinK = 16;    // smaller k: the ring search (measured faster there)
 constexpr int kTileMaxK = 40;    // largest k the cell-tile search takes
-constexpr int kTileAlpha = 5;    // block population that selects a level, in units of k+1 (measured:
-                                 // 4 to 5.5 within noise on 4M superquadrics at k = 40)
-constexpr int kTileSparse = 3;       // a finer block below kTileSparse/4 * (k+1) points: the ring search
+constexpr int kTileAlpha = 6;    // block population that selects a level, in units of k+1 (measured on
+                                 // 4M superquadrics at k = 40, with the sparse rule below: 5 to 7 within
+                                 // 2 %, 4 and 8 slower)
+constexpr int kTileSparse = 2;       // a finer block below (k+1)/kTileSparse points: the ring search (measured
+                                      // on 4M superquadrics at k = 40: (k+1)/2 and 0.6(k+1) best, 0.75(k+1)
+                                      // 8 % slower, 0.45(k+1) and below 15 % slower: its long searches return)
 constexpr int kTileMaxBlock = 6144;   // larger blocks: the ring search (one warp would hold the search's end)
 constexpr int kTileClasses = 6;       // batch classes by block size (>= 4096, 2048, 1024, 512, 256, less)
 
@@ -63,7 +66,7 @@ struct TileArgs {
     unsigned long long* n_ring;       // their count
     int thr;                          // kTileAlpha * (k+1)
     int maxblock;                     // kTileMaxBlock
-    int sparse;                       // kTileSparse * (k+1) / 4
+    int sparse;                       // (k+1) / kTileSparse
     uint32_t* qarr;                   // [n] the units' queries, grouped by unit (k_tile_gather)
     unsigned long long* n_q;          // queries written to qarr
     uint2* batch;                     // [bcap] (unit, first query in qarr), largest blocks first
