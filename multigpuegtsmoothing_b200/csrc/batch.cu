@@ -35,6 +35,7 @@
 #include "knn_common.cuh"
 #include "knn_search.cuh"
 #include "knn_select.cuh"
+#include "knn_tile.cuh"
 
 using egt::KnnArgs;
 using egt::LevelDev;
@@ -482,6 +483,49 @@ egt_status launch_compact_batch(egt_batch* b, cudaStream_t st) {
 }
 
 // Blocks of one resident wave of k_knn_batch<S>.
+// Largest cell population of each cloud and level (the cell-tile search's
+// oversized-cell check): block (cloud, level).
+__global__ void __launch_bounds__(256) k_maxpop_batch(const KnnArgs* __restrict__ desc) {
+    const KnnArgs& a = desc[blockIdx.x];
+    const LevelDev& LV = a.lv[blockIdx.y];
+    int v = 0;
+    for (int i = threadIdx.x; i < LV.ncells; i += blockDim.x) v = max(v, LV.cell_start[i + 1] - LV.cell_start[i]);
+    v = __reduce_max_sync(0xffffffffu, v);
+    if ((threadIdx.x & 31) == 0 && v > 0) atomicMax(&a.counters[kCtrMaxPop + blockIdx.y], (unsigned long long)v);
+}
+
+// The ring search of the queries in `list` (indices over all clouds' points),
+// one query per warp.
+template <int S>
+__global__ void __launch_bounds__(kWarps * 32) k_knn_list_batch(const KnnArgs* __restrict__ desc,
+                                                                const uint16_t* __restrict__ cloud,
+                                                                const int* __restrict__ list,
+                                                                const unsigned long long* __restrict__ n_list,
+                                                                unsigned long long* __restrict__ work) {
+    __shared__ int s_pref[kWarps][32];
+    __shared__ int s_start[kWarps][32];
+    __shared__ float s_md[kWarps][32 * S];
+    __shared__ int s_mp[kWarps][32 * S];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned long long n = *n_list;
+    for (;;) {
+        unsigned long long j = 0;
+        if (lane == 0) j = atomicAdd(work, 1ull);
+        j = __shfl_sync(0xffffffffu, j, 0);
+        if (j >= n) break;
+        const int i = list[j];
+        const KnnArgs& a = desc[cloud[i]];
+        const int q = i - (int)a.gbase;
+        const NormParams np = *a.np;
+        WarpList<S> L;
+        bool invalid, rerun;
+        const int reached = plain_query<true, S>(a, np, q, a.p4[q], L, invalid, lane, s_pref[w], s_start[w], s_md[w],
+                                                 s_mp[w], rerun);
+        write_query<S>(a, q, L, invalid, reached, lane);
+        if (rerun && lane == 0) atomicAdd(&a.counters[kCtrExactRerun], 1ull);
+    }
+}
+
 template <int S>
 egt_status knn_wave(int device, unsigned* out) {
     static std::mutex mu;
@@ -549,6 +593,30 @@ egt_status set_chunk(egt_batch* b, int chunk) {
     return EGT_OK;
 }
 
+// The cell-tile search over every cloud (clouds whose k lies outside
+// [kTileMinK, kTileMaxK] run the ring search), then the ring search of the
+// queries it could not certify.
+template <int S>
+egt_status knn_batch_tile(egt_batch* b, cudaStream_t st) {
+    TileArgs t;
+    EGT_TRY(tile_prepare(b->h, &t));
+    t.desc = b->d_desc;
+    t.cloud_of = b->d_cloud;
+    t.npts = (int)b->N;
+    EGT_CUDA_TRY(cudaMemset2DAsync(b->d_ctr + kCtrMaxPop, sizeof(unsigned long long) * kCtrWords, 0,
+                                   kMaxLevels * sizeof(unsigned long long), b->count, st));
+    k_maxpop_batch<<<dim3(b->count, kMaxLevels), 256, 0, st>>>(b->d_desc);
+    EGT_LAUNCH_CHECK();
+    KnnArgs none{};  // each cloud's arguments come from its descriptor
+    EGT_TRY(tile_launch<true>(none, t, st));
+    unsigned G = 0;
+    EGT_TRY(kernel_wave(k_knn_list_batch<S>, b->cfg.device, &G));
+    k_knn_list_batch<S><<<G, kWarps * 32, 0, st>>>(b->d_desc, b->d_cloud, t.ring2, t.n_ring2,
+                                                   b->h->d_counters + kCtrTileRingWork);
+    EGT_LAUNCH_CHECK();
+    return EGT_OK;
+}
+
 egt_status knn_batch(egt_batch* b) {
     cudaStream_t st = b->h->stream;
     EGT_TRY(set_chunk(b, b->chunk > 0 ? b->chunk : kChunk));
@@ -560,7 +628,18 @@ egt_status knn_batch(egt_batch* b) {
                                    sizeof(unsigned long long), b->count, st));
     EGT_CUDA_TRY(cudaEventRecord(b->h->ev[2], st));
     const int kk = b->kmax;
-    if (kk + 1 <= 32) EGT_TRY(run_knn_batch_s<1>(b, st));
+    bool tile = b->cfg.knn_mode == EGT_KNN_TILE;
+    if (tile) {
+        tile = false;
+        for (int c = 0; c < b->count; c++) tile |= b->k[c] >= kTileMinK && b->k[c] <= kTileMaxK;
+    }
+    if (tile) {
+        if (kk + 1 <= 32) EGT_TRY(knn_batch_tile<1>(b, st));
+        else if (kk + 1 <= 64) EGT_TRY(knn_batch_tile<2>(b, st));
+        else if (kk + 1 <= 96) EGT_TRY(knn_batch_tile<3>(b, st));
+        else if (kk + 1 <= 128) EGT_TRY(knn_batch_tile<4>(b, st));
+        else EGT_TRY(knn_batch_tile<8>(b, st));
+    } else if (kk + 1 <= 32) EGT_TRY(run_knn_batch_s<1>(b, st));
     else if (kk + 1 <= 64) EGT_TRY(run_knn_batch_s<2>(b, st));
     else if (kk + 1 <= 96) EGT_TRY(run_knn_batch_s<3>(b, st));
     else if (kk + 1 <= 128) EGT_TRY(run_knn_batch_s<4>(b, st));

@@ -848,103 +848,16 @@ static egt_status knn_search(const KnnArgs& a, bool select, cudaStream_t st) {
     return launch_select<3>(as, st);
 }
 
-// Working buffers of the cell-tile search (knn_tile.cuh) for handle h.
-static egt_status tile_prepare(egt_handle* h, int k, TileArgs* t) {
-    const int64_t n = h->n;
-    const int words = (int)((n + 31) / 32);
-    const int64_t bcap = n + n / 16 + 1;
-    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const size_t b_lq = al((size_t)n), b_bits = al((size_t)kMaxLevels * words * 4), b_n4 = al(4 * (size_t)n);
-    const size_t b_batch = al(8 * (size_t)bcap), b_bcnt = al((size_t)bcap), b_ctr = 256;
-    const size_t need = b_ctr + b_lq + b_bits + 5 * b_n4 + b_batch + b_bcnt + b_lq;
-    if (h->tile_bytes < need) {
-        dev_free(h, h->tile_mem);
-        h->tile_mem = nullptr;
-        h->tile_bytes = 0;
-        EGT_CUDA_TRY(dev_alloc(h, &h->tile_mem, need));
-        h->tile_bytes = need;
-    }
-    unsigned char* m = static_cast<unsigned char*>(h->tile_mem);
-    unsigned long long* tctr = reinterpret_cast<unsigned long long*>(m);  // class counts and fills
-    t->cls_n = tctr;
-    t->cls_fill = tctr + kTileClasses;
-    m += b_ctr;
-    t->lq = m;
-    m += b_lq;
-    t->unit_bits = reinterpret_cast<uint32_t*>(m);
-    m += b_bits;
-    t->words = words;
-    t->units = reinterpret_cast<uint32_t*>(m);
-    m += b_n4;
-    t->ring = reinterpret_cast<int*>(m);
-    m += b_n4;
-    t->ring2 = reinterpret_cast<int*>(m);
-    m += b_n4;
-    t->qarr = reinterpret_cast<uint32_t*>(m);
-    m += b_n4;
-    t->ucnt = reinterpret_cast<uint32_t*>(m);
-    m += b_n4;
-    t->batch = reinterpret_cast<uint2*>(m);
-    m += b_batch;
-    t->bcnt = m;
-    m += b_bcnt;
-    t->ucls = m;
-    t->bcap = (int)bcap;
-    t->n_units = h->d_counters + kCtrTileUnits;
-    t->unit_work = h->d_counters + kCtrTileWork;
-    t->n_ring = h->d_counters + kCtrSelFallback;
-    t->n_q = h->d_counters + kCtrTileQ;
-    t->n_ring2 = h->d_counters + kCtrTileRing2;
-    t->ring_work = h->d_counters + kCtrTileRingWork1;
-    t->thr = kTileAlpha * (k + 1);
-    t->maxblock = kTileMaxBlock;
-    t->sparse = (k + 1) / kTileSparse;
-    cudaStream_t st = h->stream;
-    EGT_CUDA_TRY(cudaMemsetAsync(t->unit_bits, 0, b_bits, st));
-    EGT_CUDA_TRY(cudaMemsetAsync(tctr, 0, b_ctr, st));
-    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrTileUnits, 0, 8 * sizeof(unsigned long long), st));
-    return EGT_OK;
-}
-
 // The cell-tile search of every query, then the ring search of the queries
 // it could not certify (the counters must be reset).
 static egt_status tile_search(egt_handle* h, const KnnArgs& a, cudaStream_t st) {
     TileArgs t;
-    EGT_TRY(tile_prepare(h, a.k, &t));
+    EGT_TRY(tile_prepare(h, &t));
+    t.desc = nullptr;
+    t.cloud_of = nullptr;
+    t.npts = a.n;
     EGT_TRY(level_maxpop(h));  // condition (4)
-    const unsigned T = 256;
-    k_tile_assign<<<(unsigned)((a.n + T - 1) / T), T, 0, st>>>(a, t);
-    EGT_LAUNCH_CHECK();
-    const unsigned Gu = (unsigned)std::min<int64_t>(4096, (a.n + T - 1) / T);
-    k_tile_count<<<Gu, T, 0, st>>>(a, t);
-    EGT_LAUNCH_CHECK();
-    k_tile_gather<<<Gu, T, 0, st>>>(a, t);
-    EGT_LAUNCH_CHECK();
-    static std::atomic<uint64_t> attr_set{0};  // per device
-    int dev = 0;
-    EGT_CUDA_TRY(cudaGetDevice(&dev));
-    if (!(attr_set.load() >> (dev & 63) & 1)) {
-        EGT_CUDA_TRY(cudaFuncSetAttribute(k_knn_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
-        attr_set.fetch_or(uint64_t(1) << (dev & 63));
-    }
-    static std::mutex mu;
-    static std::map<int, unsigned> waves;  // per device: blocks of one resident wave
-    unsigned G = 0;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        auto it = waves.find(dev);
-        if (it != waves.end()) G = it->second;
-    }
-    if (!G) {
-        int sms = 0, per = 0;
-        EGT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        EGT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_knn_tile, kTileWarps * 32, kTileSmem));
-        G = (unsigned)std::max(1, sms * std::max(per, 1));
-        std::lock_guard<std::mutex> lock(mu);
-        waves[dev] = G;
-    }
-    k_knn_tile<<<G, kTileWarps * 32, kTileSmem, st>>>(a, t);
-    EGT_LAUNCH_CHECK();
+    EGT_TRY(tile_launch<false>(a, t, st));
     KnnArgs ar = a;
     ar.qmap = t.ring2;
     ar.n_dev = t.n_ring2;

@@ -35,6 +35,8 @@
 // holds at least kTileAlpha * (k+1) points (k_tile_assign); every cell that
 // has queries at its level becomes one unit of work.
 #pragma once
+#include <map>
+#include <mutex>
 #include "knn_search.cuh"
 #include "proposal.cuh"
 
@@ -59,17 +61,15 @@ struct TileArgs {
     uint8_t* lq;                      // [n] level each query is searched at (0xff: ring search)
     uint32_t* unit_bits;              // [kMaxLevels][words] cells that already have a unit
     int words;                        // words per level
-    uint32_t* units;                  // [n] level << 29 | cell index
+    unsigned long long* units;        // [n] cloud << 40 | level << 32 | cell index
     unsigned long long* n_units;      // units written by k_tile_assign
     unsigned long long* unit_work;    // next unit to claim
     int* ring;                        // [n] queries for the ring search
     unsigned long long* n_ring;       // their count
-    int thr;                          // kTileAlpha * (k+1)
     int maxblock;                     // kTileMaxBlock
-    int sparse;                       // (k+1) / kTileSparse
     uint32_t* qarr;                   // [n] the units' queries, grouped by unit (k_tile_gather)
     unsigned long long* n_q;          // queries written to qarr
-    uint2* batch;                     // [bcap] (unit, first query in qarr), largest blocks first
+    uint2* batch;                     // [bcap] (unit index, first query in qarr), largest blocks first
     uint8_t* bcnt;                    // [bcap] queries in each batch (1..16)
     int bcap;                         // n + n/16 + 1 >= units + queries/16
     uint32_t* ucnt;                   // [n] queries of each unit
@@ -79,7 +79,30 @@ struct TileArgs {
     int* ring2;                       // [n] queries the tile search could not certify
     unsigned long long* n_ring2;      // their count
     unsigned long long* ring_work;    // next query of `ring` for the tile kernel's ring search
+    // Several clouds (egt_batch): the search arguments of each cloud, and each
+    // point's cloud.  Queries, lq and the ring lists then use indices over
+    // all clouds' points; a single cloud passes its own arguments instead.
+    const KnnArgs* desc;
+    const uint16_t* cloud_of;
+    int npts;                         // points of all clouds
 };
+
+// The search arguments of cloud c: the kernel's own (one cloud), or the
+// cloud's descriptor.
+template <bool kBatch>
+__device__ __forceinline__ const KnnArgs& tile_args(const KnnArgs& a, const TileArgs& t, int c) {
+    if constexpr (kBatch) return t.desc[c];
+    else return a;
+}
+
+__device__ __forceinline__ unsigned long long unit_code(int c, int l, int ci) {
+    return ((unsigned long long)c << 40) | ((unsigned long long)l << 32) | (unsigned)ci;
+}
+__device__ __forceinline__ void unit_parts(unsigned long long code, int& c, int& l, int& ci) {
+    c = (int)(code >> 40);
+    l = (int)((code >> 32) & 0xffu);
+    ci = (int)(code & 0xffffffffu);
+}
 
 // Shared memory of one warp (both halves).
 constexpr size_t kTileWarpBytes = (size_t)kTileBins * 32 * 4   // bucket counts, then offsets [bucket][lane]
@@ -116,20 +139,38 @@ __device__ __forceinline__ void warp_append(bool flag, uint32_t v, uint32_t* lis
     if (flag) list[base + __popc(m & ((1u << lane) - 1u))] = v;
 }
 
+__device__ __forceinline__ void warp_append64(bool flag, unsigned long long v, unsigned long long* list,
+                                              unsigned long long* count, int lane) {
+    const unsigned m = __ballot_sync(0xffffffffu, flag);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (flag) list[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
 // Level and unit of every query; queries that no level selects (or every
-// query when the admission threshold can cut lists) go to the ring search.
+// query when the admission threshold can cut lists, or when k is outside
+// [kTileMinK, kTileMaxK]) go to the ring search.  i runs over the points of
+// all clouds (their sorted order).
+template <bool kBatch>
 __global__ void __launch_bounds__(256) k_tile_assign(KnnArgs a, TileArgs t) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    const bool in = q < a.n;
+    const bool in = i < t.npts;
+    const int c = (kBatch && in) ? (int)t.cloud_of[i] : 0;
+    const KnnArgs& A = tile_args<kBatch>(a, t, c);
+    const int q = i - (int)A.gbase;
     int lsel = -1, ci = -1;
     // thres > 4 exceeds every squared distance of the unit cube: all admitted
-    if (in && a.np->thres > 4.0f) {
-        const uint32_t c0 = __float_as_uint(a.p4[q].w);
+    if (in && A.k >= kTileMinK && A.k <= kTileMaxK && A.np->thres > 4.0f) {
+        const int thr = kTileAlpha * (A.k + 1), sparse = (A.k + 1) / kTileSparse;
+        const uint32_t c0 = __float_as_uint(A.p4[q].w);
         const int cx0 = c0 & 1023u, cy0 = (c0 >> 10) & 1023u, cz0 = (c0 >> 20) & 1023u;
         int prev = INT_MAX;  // population of the block one level finer
         for (int l = 0; l < kMaxLevels && lsel < 0; l++) {
-            const LevelDev& LV = a.lv[l];
+            const LevelDev& LV = A.lv[l];
             const int cx = cx0 >> l, cy = cy0 >> l, cz = cz0 >> l;
             int pop = 0;
 #pragma unroll
@@ -137,25 +178,34 @@ __global__ void __launch_bounds__(256) k_tile_assign(KnnArgs a, TileArgs t) {
                 const int2 g = row_points(LV, cx - 1, cx + 1, cy + r % 3 - 1, cz + r / 3 - 1);
                 pop += g.y - g.x;
             }
-            if (pop >= t.thr) {
+            if (pop >= thr) {
                 // kMaxLevels: a block too large, or a query alone in its finer
                 // block -- the ring search (such a query's k nearest lie far
                 // off, beyond the block, and its search climbs high)
-                lsel = pop <= t.maxblock && prev >= t.sparse ? l : kMaxLevels;
+                lsel = pop <= t.maxblock && prev >= sparse ? l : kMaxLevels;
                 if (lsel == l) ci = cell_index(LV, cx, cy, cz);
             }
             prev = pop;
         }
     }
     if (lsel >= kMaxLevels || ci < 0) lsel = -1;  // ci < 0 cannot happen: the query's own cell is occupied
-    warp_append(in && lsel < 0, (uint32_t)q, reinterpret_cast<uint32_t*>(t.ring), t.n_ring, lane);
-    if (in) t.lq[q] = lsel < 0 ? (uint8_t)0xff : (uint8_t)lsel;
+    // The tile kernel runs the ring search of the queries its k range takes
+    // but no level selects (few, some long: they overlap the batches); the
+    // clouds outside that range run it in the launch after the tile kernel,
+    // at the ring search's own occupancy.
+    const bool ring = in && lsel < 0;
+    const bool early = A.k >= kTileMinK && A.k <= kTileMaxK;
+    warp_append(ring && early, (uint32_t)i, reinterpret_cast<uint32_t*>(t.ring), t.n_ring, lane);
+    warp_append(ring && !early, (uint32_t)i, reinterpret_cast<uint32_t*>(t.ring2), t.n_ring2, lane);
+    if (in) t.lq[i] = lsel < 0 ? (uint8_t)0xff : (uint8_t)lsel;
     bool fresh = false;
     if (lsel >= 0) {
-        const uint32_t bit = 1u << (ci & 31);
-        fresh = !(atomicOr(t.unit_bits + (size_t)lsel * t.words + (ci >> 5), bit) & bit);
+        // a cell is named by the first position of its points in the level's order
+        const int first = (int)A.gbase + A.lv[lsel].cell_start[ci];
+        const uint32_t bit = 1u << (first & 31);
+        fresh = !(atomicOr(t.unit_bits + (size_t)lsel * t.words + (first >> 5), bit) & bit);
     }
-    warp_append(fresh, ((uint32_t)lsel << 29) | (uint32_t)ci, t.units, t.n_units, lane);
+    warp_append64(fresh, unit_code(c, lsel, ci), t.units, t.n_units, lane);
 }
 
 // Class of a block of `pop` candidates: larger blocks are searched first, and
@@ -167,28 +217,31 @@ __device__ __forceinline__ int tile_class(int pop) {
 
 // Per unit (one warp per unit, grid-stride): its query count and block class,
 // and the batch count of each class.
+template <bool kBatch>
 __global__ void __launch_bounds__(256) k_tile_count(KnnArgs a, TileArgs t) {
     const int lane = threadIdx.x & 31;
     const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nw = (int)((gridDim.x * blockDim.x) >> 5);
     const unsigned long long nu = *t.n_units;
     for (unsigned long long u = gw; u < nu; u += nw) {
-        const uint32_t code = t.units[u];
-        const int l = (int)(code >> 29), ci = (int)(code & 0x1fffffffu);
-        const LevelDev& LV = a.lv[l];
+        int c, l, ci;
+        unit_parts(t.units[u], c, l, ci);
+        const KnnArgs& A = tile_args<kBatch>(a, t, c);
+        const LevelDev& LV = A.lv[l];
         const int* order = l ? LV.order : nullptr;
         const int cs = LV.cell_start[ci], ce = LV.cell_start[ci + 1];
+        const uint8_t* lq = t.lq + A.gbase;
         int cnt = 0;
         for (int s = cs; s < ce; s += 32) {
             bool sel = false;
             if (s + lane < ce) {
                 const int qq = order ? order[s + lane] : s + lane;
-                sel = t.lq[qq] == (uint8_t)l;
+                sel = lq[qq] == (uint8_t)l;
             }
             cnt += __popc(__ballot_sync(0xffffffffu, sel));
         }
         const int p0 = order ? order[cs] : cs;
-        const uint32_t cc = __float_as_uint(a.p4[p0].w);
+        const uint32_t cc = __float_as_uint(A.p4[p0].w);
         const int cx = (int)(cc & 1023u) >> l, cy = (int)((cc >> 10) & 1023u) >> l, cz = (int)((cc >> 20) & 1023u) >> l;
         int pop = 0;
         if (lane < 9) {
@@ -207,6 +260,7 @@ __global__ void __launch_bounds__(256) k_tile_count(KnnArgs a, TileArgs t) {
 
 // Compacts each unit's queries into qarr and cuts them into batches of up to
 // 16 (one warp per unit, grid-stride), the batches ordered by class.
+template <bool kBatch>
 __global__ void __launch_bounds__(256) k_tile_gather(KnnArgs a, TileArgs t) {
     const int lane = threadIdx.x & 31;
     const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -225,11 +279,13 @@ __global__ void __launch_bounds__(256) k_tile_gather(KnnArgs a, TileArgs t) {
         coff = incl - v;
     }
     for (unsigned long long u = gw; u < nu; u += nw) {
-        const uint32_t code = t.units[u];
-        const int l = (int)(code >> 29), ci = (int)(code & 0x1fffffffu);
-        const LevelDev& LV = a.lv[l];
+        int c, l, ci;
+        unit_parts(t.units[u], c, l, ci);
+        const KnnArgs& A = tile_args<kBatch>(a, t, c);
+        const LevelDev& LV = A.lv[l];
         const int* order = l ? LV.order : nullptr;
         const int cs = LV.cell_start[ci], ce = LV.cell_start[ci + 1];
+        const uint8_t* lq = t.lq + A.gbase;
         const int cnt = (int)t.ucnt[u], cls = (int)t.ucls[u];
         const int nbat = (cnt + 15) >> 4;
         const unsigned long long base = __shfl_sync(0xffffffffu, coff, cls);
@@ -246,14 +302,14 @@ __global__ void __launch_bounds__(256) k_tile_gather(KnnArgs a, TileArgs t) {
             int qq = -1;
             if (s + lane < ce) {
                 qq = order ? order[s + lane] : s + lane;
-                sel = t.lq[qq] == (uint8_t)l;
+                sel = lq[qq] == (uint8_t)l;
             }
             const unsigned m = __ballot_sync(0xffffffffu, sel);
             if (sel) t.qarr[qb + w + __popc(m & ((1u << lane) - 1u))] = (uint32_t)qq;
             w += __popc(m);
         }
         for (int j = lane; j < nbat; j += 32) {
-            t.batch[bb + j] = make_uint2(code, (uint32_t)(qb + 16 * j));
+            t.batch[bb + j] = make_uint2((uint32_t)u, (uint32_t)(qb + 16 * j));
             t.bcnt[bb + j] = (uint8_t)min(16, cnt - 16 * j);
         }
     }
@@ -355,9 +411,8 @@ __device__ __forceinline__ void tile_stream16(const TileUnit& U, bool live, int 
 
 // Sets up a new unit for the lanes with `take` (both halves call it; a half
 // with take = false keeps its unit).
-__device__ __forceinline__ void tile_unit_setup(const KnnArgs& a, const NormParams& np, uint32_t code, bool take,
+__device__ __forceinline__ void tile_unit_setup(const KnnArgs& a, const NormParams& np, int l, int ci, bool take,
                                                 int hl, int hf, int* s_pref, int* s_start, TileUnit& U) {
-    const int l = (int)(code >> 29), ci = (int)(code & 0x1fffffffu);
     int2 rg = make_int2(0, 0);
     int cx = 0, cy = 0, cz = 0;
     const int* order = nullptr;
@@ -386,6 +441,7 @@ __device__ __forceinline__ void tile_unit_setup(const KnnArgs& a, const NormPara
 
 // Persistent: each half-warp claims batches (up to 16 queries of one unit)
 // one at a time; both halves run their batches together.
+template <bool kBatch>
 __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArgs t) {
     extern __shared__ __align__(16) unsigned char s_tile[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -397,8 +453,6 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
     int* s_pref = reinterpret_cast<int*>(reinterpret_cast<float4*>(bpos + (size_t)kTileCap * 32) + 32) + 32 * hf;
     int* s_start = s_pref + 16;
     uint32_t* hcol = hist + lane;
-    const NormParams np = *a.np;
-    const int k = a.k;
     unsigned long long evals = 0;
     unsigned maxlev = 0;
     // First the ring search (k_knn_plain's code, one query per warp) of the
@@ -412,14 +466,22 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
     float* r_md = reinterpret_cast<float*>(r_start + 32);
     int* r_mp = reinterpret_cast<int*>(r_md + 64);
     unsigned reruns = 0;
-    auto ring_query = [&](int q) {
+    auto ring_query = [&](int i) {  // i: over all clouds' points
+        const int c = kBatch ? (int)t.cloud_of[i] : 0;
+        const KnnArgs& A = tile_args<kBatch>(a, t, c);
+        const int q = i - (int)A.gbase;
+        const NormParams np = *A.np;
         WarpList<2> L;
         bool invalid, rerun;
-        const int reached = plain_query<true, 2>(a, np, q, a.p4[q], L, invalid, lane, r_pref, r_start, r_md, r_mp,
+        const int reached = plain_query<true, 2>(A, np, q, A.p4[q], L, invalid, lane, r_pref, r_start, r_md, r_mp,
                                                  rerun);
-        write_query<2>(a, q, L, invalid, reached, lane);
-        reruns += rerun ? 1u : 0u;
-        evals += L.ev;
+        write_query<2>(A, q, L, invalid, reached, lane);
+        if constexpr (kBatch) {
+            if (rerun && lane == 0) atomicAdd(&A.counters[kCtrExactRerun], 1ull);
+        } else {
+            reruns += rerun ? 1u : 0u;
+            evals += L.ev;
+        }
     };
     {
         const unsigned long long n_r = *t.n_ring;
@@ -433,7 +495,6 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
         __syncwarp();
     }
     for (int b = 0; b < kTileBins; b++) hcol[b * 32] = 0u;
-    const float4* __restrict__ p4 = a.p4;
     TileUnit U;
     U.seq.incl = INT_MAX;
     U.seq.cs = 0;
@@ -455,7 +516,13 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
         const long long bi = take ? (long long)c : 0;
         const uint2 bd = take ? t.batch[bi] : make_uint2(0u, 0u);
         const int nq = take ? (int)t.bcnt[bi] : 0;
-        tile_unit_setup(a, np, bd.x, take, hl, hf, s_pref, s_start, U);
+        int uc = 0, ul = 0, uci = 0;
+        unit_parts(t.units[bd.x], uc, ul, uci);
+        const KnnArgs& A = tile_args<kBatch>(a, t, uc);  // the half's cloud
+        const NormParams np = *A.np;
+        const int k = A.k;
+        const float4* __restrict__ p4 = A.p4;
+        tile_unit_setup(A, np, ul, uci, take, hl, hf, s_pref, s_start, U);
         const bool act = hl < nq;
         const int q = act ? (int)t.qarr[bd.y + hl] : -1;
         const float4 pq = act ? p4[q] : make_float4(3e18f, 3e18f, 3e18f, 0.f);
@@ -577,21 +644,26 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
             // (4) no oversized cell on the visited levels
             if (ok)
                 for (int L = 0; L <= max(sf - 1, 0) && ok; L++)
-                    ok = a.counters[kCtrMaxPop + L] < (unsigned long long)a.max_pts;
+                    ok = A.counters[kCtrMaxPop + L] < (unsigned long long)A.max_pts;
             reached = max(sf - 1, 0);
         }
         if (ok) {
-            int* row = a.lists + (size_t)q * k;
+            int* row = A.lists + (size_t)q * k;
             for (int i = 0; i < k; i++) row[i] = tile_point(bpos[tile_slot(i + (i >= self), lane)], U, s_pref, s_start);
-            if (a.kth_out) a.kth_out[q] = kth;
-            if (a.qlevel) a.qlevel[q] = (uint8_t)reached;
-            maxlev = max(maxlev, (unsigned)reached);
+            if (A.kth_out) A.kth_out[q] = kth;
+            if (A.qlevel) A.qlevel[q] = (uint8_t)reached;
+            if constexpr (kBatch) {
+                atomicMax(&A.counters[kCtrMaxLevel], (unsigned long long)reached);
+            } else {
+                maxlev = max(maxlev, (unsigned)reached);
+            }
         }
-        if (hl == 0) evals += (unsigned long long)total * nq;
-        warp_append(act && !ok, (uint32_t)q, reinterpret_cast<uint32_t*>(t.ring2), t.n_ring2, lane);
+        if (!kBatch && hl == 0) evals += (unsigned long long)total * nq;
+        warp_append(act && !ok, (uint32_t)(A.gbase + q), reinterpret_cast<uint32_t*>(t.ring2), t.n_ring2, lane);
 #pragma unroll 8
         for (int b = 0; b < kTileBins; b++) hcol[b * 32] = 0u;
     }
+    if constexpr (kBatch) return;  // per-cloud counters were updated as the queries finished
     maxlev = __reduce_max_sync(0xffffffffu, maxlev);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
@@ -600,6 +672,107 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
         if (evals) atomicAdd(&a.counters[kCtrEvals], evals);
         if (maxlev) atomicMax(&a.counters[kCtrMaxLevel], (unsigned long long)maxlev);
     }
+}
+
+
+// Working buffers of the cell-tile search for the handle's n points (all
+// clouds' points for a batch), and its counters reset.
+inline egt_status tile_prepare(egt_handle* h, TileArgs* t) {
+    const int64_t n = h->n;
+    const int words = (int)((n + 31) / 32);
+    const int64_t bcap = n + n / 16 + 1;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t b_lq = al((size_t)n), b_bits = al((size_t)kMaxLevels * words * 4), b_n4 = al(4 * (size_t)n);
+    const size_t b_n8 = al(8 * (size_t)n);
+    const size_t b_batch = al(8 * (size_t)bcap), b_bcnt = al((size_t)bcap), b_ctr = 256;
+    const size_t need = b_ctr + b_lq + b_bits + b_n8 + 4 * b_n4 + b_batch + b_bcnt + b_lq;
+    if (h->tile_bytes < need) {
+        dev_free(h, h->tile_mem);
+        h->tile_mem = nullptr;
+        h->tile_bytes = 0;
+        EGT_CUDA_TRY(dev_alloc(h, &h->tile_mem, need));
+        h->tile_bytes = need;
+    }
+    unsigned char* m = static_cast<unsigned char*>(h->tile_mem);
+    unsigned long long* tctr = reinterpret_cast<unsigned long long*>(m);  // class counts and fills
+    t->cls_n = tctr;
+    t->cls_fill = tctr + kTileClasses;
+    m += b_ctr;
+    t->lq = m;
+    m += b_lq;
+    t->unit_bits = reinterpret_cast<uint32_t*>(m);
+    m += b_bits;
+    t->words = words;
+    t->units = reinterpret_cast<unsigned long long*>(m);
+    m += b_n8;
+    t->ring = reinterpret_cast<int*>(m);
+    m += b_n4;
+    t->ring2 = reinterpret_cast<int*>(m);
+    m += b_n4;
+    t->qarr = reinterpret_cast<uint32_t*>(m);
+    m += b_n4;
+    t->ucnt = reinterpret_cast<uint32_t*>(m);
+    m += b_n4;
+    t->batch = reinterpret_cast<uint2*>(m);
+    m += b_batch;
+    t->bcnt = m;
+    m += b_bcnt;
+    t->ucls = m;
+    t->bcap = (int)bcap;
+    t->n_units = h->d_counters + kCtrTileUnits;
+    t->unit_work = h->d_counters + kCtrTileWork;
+    t->n_ring = h->d_counters + kCtrSelFallback;
+    t->n_q = h->d_counters + kCtrTileQ;
+    t->n_ring2 = h->d_counters + kCtrTileRing2;
+    t->ring_work = h->d_counters + kCtrTileRingWork1;
+    t->maxblock = kTileMaxBlock;
+    t->desc = nullptr;
+    t->cloud_of = nullptr;
+    t->npts = (int)n;
+    cudaStream_t st = h->stream;
+    EGT_CUDA_TRY(cudaMemsetAsync(t->unit_bits, 0, b_bits, st));
+    EGT_CUDA_TRY(cudaMemsetAsync(tctr, 0, b_ctr, st));
+    EGT_CUDA_TRY(cudaMemsetAsync(h->d_counters + kCtrTileUnits, 0, 8 * sizeof(unsigned long long), st));
+    return EGT_OK;
+}
+
+// Assignment, batching and the tile kernel (with the ring search of the
+// queries no level selected); the uncertified queries are left in t.ring2.
+template <bool kBatch>
+egt_status tile_launch(const KnnArgs& a, const TileArgs& t, cudaStream_t st) {
+    const unsigned T = 256;
+    const int64_t npts = t.npts;
+    k_tile_assign<kBatch><<<(unsigned)((npts + T - 1) / T), T, 0, st>>>(a, t);
+    EGT_LAUNCH_CHECK();
+    const unsigned Gu = (unsigned)std::min<int64_t>(4096, (npts + T - 1) / T);
+    k_tile_count<kBatch><<<Gu, T, 0, st>>>(a, t);
+    EGT_LAUNCH_CHECK();
+    k_tile_gather<kBatch><<<Gu, T, 0, st>>>(a, t);
+    EGT_LAUNCH_CHECK();
+    static std::mutex mu;
+    static std::map<int, unsigned> waves;  // per device: blocks of one resident wave
+    int dev = 0;
+    EGT_CUDA_TRY(cudaGetDevice(&dev));
+    unsigned G = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = waves.find(dev);
+        if (it != waves.end()) G = it->second;
+    }
+    if (!G) {
+        EGT_CUDA_TRY(cudaFuncSetAttribute(k_knn_tile<kBatch>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kTileSmem));
+        int sms = 0, per = 0;
+        EGT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        EGT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_knn_tile<kBatch>, kTileWarps * 32,
+                                                                    kTileSmem));
+        G = (unsigned)std::max(1, sms * std::max(per, 1));
+        std::lock_guard<std::mutex> lock(mu);
+        waves[dev] = G;
+    }
+    k_knn_tile<kBatch><<<G, kTileWarps * 32, kTileSmem, st>>>(a, t);
+    EGT_LAUNCH_CHECK();
+    return EGT_OK;
 }
 
 }  // namespace
