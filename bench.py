@@ -368,7 +368,7 @@ def learned_compare(capi, xyz, k, train, workload):
            "block_selection_note": "the block-selection search (EGT_KNN_SELECT) on the same cloud, same lists",
            "tile_ms": min(tile_ms), "tile_mqueries_s": n / min(tile_ms) / 1e3,
            "tile_note": "the cell-tile search (EGT_KNN_TILE, egt_knn's default; the ring search for k outside "
-                        "16..40) on the same cloud, same lists"}
+                        "16..64) on the same cloud, same lists"}
     g.close()
     p.close()
     return out

@@ -47,7 +47,7 @@ typedef struct egt_proposal egt_proposal;
 #define EGT_KNN_LEARNED 1  /* proposal-driven box search, certified rows; the ring search for the rest */
 #define EGT_KNN_SELECT 2   /* block selection, certified rows; the ring search for the rest */
 #define EGT_KNN_TILE 3     /* cell tiles (default): a cell's queries one per lane over its 3x3x3
-                              block, certified rows; the ring search for the rest.  For 16 <= k <= 40;
+                              block, certified rows; the ring search for the rest.  For 16 <= k <= 64;
                               other k use the ring search */
 
 /* Tunables.  Defaults reproduce the reference CLI (main.cpp:108-116). */

@@ -607,8 +607,11 @@ egt_status knn_batch_tile(egt_batch* b, cudaStream_t st) {
                                    kMaxLevels * sizeof(unsigned long long), b->count, st));
     k_maxpop_batch<<<dim3(b->count, kMaxLevels), 256, 0, st>>>(b->d_desc);
     EGT_LAUNCH_CHECK();
+    int kt = 0;  // the largest k the tile search takes
+    for (int c = 0; c < b->count; c++)
+        if (b->k[c] >= kTileMinK && b->k[c] <= kTileMaxK) kt = std::max(kt, b->k[c]);
     KnnArgs none{};  // each cloud's arguments come from its descriptor
-    EGT_TRY(tile_launch<true>(none, t, st));
+    EGT_TRY(tile_launch<true>(none, t, kt, st));
     unsigned G = 0;
     EGT_TRY(kernel_wave(k_knn_list_batch<S>, b->cfg.device, &G));
     k_knn_list_batch<S><<<G, kWarps * 32, 0, st>>>(b->d_desc, b->d_cloud, t.ring2, t.n_ring2,

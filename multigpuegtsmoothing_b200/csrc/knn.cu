@@ -857,7 +857,7 @@ static egt_status tile_search(egt_handle* h, const KnnArgs& a, cudaStream_t st) 
     t.cloud_of = nullptr;
     t.npts = a.n;
     EGT_TRY(level_maxpop(h));  // condition (4)
-    EGT_TRY(tile_launch<false>(a, t, st));
+    EGT_TRY(tile_launch<false>(a, t, a.k, st));
     KnnArgs ar = a;
     ar.qmap = t.ring2;
     ar.n_dev = t.n_ring2;

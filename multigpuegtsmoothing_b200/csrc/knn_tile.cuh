@@ -15,7 +15,7 @@
 //           octave of d^2 from (h/4)^2 to (4h)^2, h the level's cell side)
 //           and finds the bucket b* holding its (k+1)-th smallest;
 //   pass 2  each lane keeps the block positions (16 bits) of buckets <= b*
-//           (at most kTileCap) in bucket order (offsets from pass 1's counts);
+//           (at most tile_cap) in bucket order (offsets from pass 1's counts);
 //           their distances are computed again into the spent bucket space
 //           and the list is insertion-sorted (only candidates of one bucket
 //           are out of order).
@@ -45,9 +45,13 @@ namespace {
 
 constexpr int kTileWarps = 1;    // warps per block (one: blocks pack the SM's shared memory tightly)
 constexpr int kTileBins = 64;    // distance buckets per query: 8 per octave of d^2, (h/4)^2 to (4h)^2
-constexpr int kTileCap = 64;     // candidates kept per query (the buckets up to b*, the query included)
+// S: list registers of the in-kernel ring search (k+1 <= 32 S); it also sets
+// the candidates kept per query (the buckets up to b*, the query included).
+template <int S>
+constexpr int tile_cap() { return S <= 2 ? 64 : 96; }
 constexpr int kTileMinK = 16;    // smaller k: the ring search (measured faster there)
-constexpr int kTileMaxK = 40;    // largest k the cell-tile search takes
+constexpr int kTileMaxK = 64;    // largest k the cell-tile search takes
+constexpr int kTileMaxK2 = 40;   // largest k of the narrower form (S = 2, 64 kept candidates)
 constexpr int kTileAlpha = 6;    // block population that selects a level, in units of k+1 (measured on
                                  // 4M superquadrics at k = 40, with the sparse rule below: 5 to 7 within
                                  // 2 %, 4 and 8 slower)
@@ -105,11 +109,18 @@ __device__ __forceinline__ void unit_parts(unsigned long long code, int& c, int&
 }
 
 // Shared memory of one warp (both halves).
-constexpr size_t kTileWarpBytes = (size_t)kTileBins * 32 * 4   // bucket counts, then offsets [bucket][lane]
-                                  + (size_t)kTileCap * 32 * 2  // kept candidates' block positions [slot][lane]
-                                  + 2 * 16 * 16                // staged candidates per half (x, y, z, point)
-                                  + 2 * 2 * 16 * 4;            // range sequence scratch per half
-constexpr size_t kTileSmem = kTileWarpBytes * kTileWarps;
+// Rows of the bucket space: the buckets, then the kept candidates' distances
+// (one row each, up to tile_cap).
+template <int S>
+constexpr int tile_rows() { return kTileBins > tile_cap<S>() ? kTileBins : tile_cap<S>(); }
+
+template <int S>
+constexpr size_t tile_warp_bytes() {
+    return (size_t)tile_rows<S>() * 32 * 4         // bucket counts, offsets, then kept distances [row][lane]
+           + (size_t)tile_cap<S>() * 32 * 2        // kept candidates' block positions [slot][lane]
+           + 2 * 16 * 16                           // staged candidates per half (x, y, z, point)
+           + 2 * 2 * 16 * 4;                       // range sequence scratch per half
+}
 
 // Kept-candidate slot s of lane `lane` (16-bit entries: two lanes per bank word).
 __device__ __forceinline__ int tile_slot(int s, int lane) { return s * 32 + lane; }
@@ -441,16 +452,18 @@ __device__ __forceinline__ void tile_unit_setup(const KnnArgs& a, const NormPara
 
 // Persistent: each half-warp claims batches (up to 16 queries of one unit)
 // one at a time; both halves run their batches together.
-template <bool kBatch>
+template <bool kBatch, int S>
 __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArgs t) {
+    constexpr int kCap = tile_cap<S>();
+    constexpr size_t kWarpBytes = tile_warp_bytes<S>();
     extern __shared__ __align__(16) unsigned char s_tile[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int hl = lane & 15, hf = lane >> 4;
-    unsigned char* base = s_tile + (size_t)w * kTileWarpBytes;
+    unsigned char* base = s_tile + (size_t)w * kWarpBytes;
     uint32_t* hist = reinterpret_cast<uint32_t*>(base);
-    uint16_t* bpos = reinterpret_cast<uint16_t*>(base + (size_t)kTileBins * 32 * 4);
-    float4* chunk = reinterpret_cast<float4*>(bpos + (size_t)kTileCap * 32) + 16 * hf;
-    int* s_pref = reinterpret_cast<int*>(reinterpret_cast<float4*>(bpos + (size_t)kTileCap * 32) + 32) + 32 * hf;
+    uint16_t* bpos = reinterpret_cast<uint16_t*>(base + (size_t)tile_rows<S>() * 32 * 4);
+    float4* chunk = reinterpret_cast<float4*>(bpos + (size_t)kCap * 32) + 16 * hf;
+    int* s_pref = reinterpret_cast<int*>(reinterpret_cast<float4*>(bpos + (size_t)kCap * 32) + 32) + 32 * hf;
     int* s_start = s_pref + 16;
     uint32_t* hcol = hist + lane;
     unsigned long long evals = 0;
@@ -464,18 +477,18 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
     int* r_pref = reinterpret_cast<int*>(bpos);
     int* r_start = r_pref + 32;
     float* r_md = reinterpret_cast<float*>(r_start + 32);
-    int* r_mp = reinterpret_cast<int*>(r_md + 64);
+    int* r_mp = reinterpret_cast<int*>(r_md + 32 * S);
     unsigned reruns = 0;
     auto ring_query = [&](int i) {  // i: over all clouds' points
         const int c = kBatch ? (int)t.cloud_of[i] : 0;
         const KnnArgs& A = tile_args<kBatch>(a, t, c);
         const int q = i - (int)A.gbase;
         const NormParams np = *A.np;
-        WarpList<2> L;
+        WarpList<S> L;
         bool invalid, rerun;
-        const int reached = plain_query<true, 2>(A, np, q, A.p4[q], L, invalid, lane, r_pref, r_start, r_md, r_mp,
+        const int reached = plain_query<true, S>(A, np, q, A.p4[q], L, invalid, lane, r_pref, r_start, r_md, r_mp,
                                                  rerun);
-        write_query<2>(A, q, L, invalid, reached, lane);
+        write_query<S>(A, q, L, invalid, reached, lane);
         if constexpr (kBatch) {
             if (rerun && lane == 0) atomicAdd(&A.counters[kCtrExactRerun], 1ull);
         } else {
@@ -550,7 +563,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
             cum += c;
             if (bstar < 0 && cum >= k + 2) { bstar = b; m = cum; }
         }
-        bool ok = act && bstar >= 0 && bstar < kTileBins - 1 && m <= kTileCap;
+        bool ok = act && bstar >= 0 && bstar < kTileBins - 1 && m <= kCap;
         const float T = ok ? __uint_as_float(lo + ((uint32_t)(bstar + 1) << 20)) : 0.0f;
         // pass 2: the candidates of buckets <= b*, in bucket order
         tile_stream16(U, take, steps, p4, chunk, hl, hf, [&](int st) {
@@ -738,17 +751,9 @@ inline egt_status tile_prepare(egt_handle* h, TileArgs* t) {
 
 // Assignment, batching and the tile kernel (with the ring search of the
 // queries no level selected); the uncertified queries are left in t.ring2.
-template <bool kBatch>
-egt_status tile_launch(const KnnArgs& a, const TileArgs& t, cudaStream_t st) {
-    const unsigned T = 256;
-    const int64_t npts = t.npts;
-    k_tile_assign<kBatch><<<(unsigned)((npts + T - 1) / T), T, 0, st>>>(a, t);
-    EGT_LAUNCH_CHECK();
-    const unsigned Gu = (unsigned)std::min<int64_t>(4096, (npts + T - 1) / T);
-    k_tile_count<kBatch><<<Gu, T, 0, st>>>(a, t);
-    EGT_LAUNCH_CHECK();
-    k_tile_gather<kBatch><<<Gu, T, 0, st>>>(a, t);
-    EGT_LAUNCH_CHECK();
+template <bool kBatch, int S>
+egt_status tile_kernel_launch(const KnnArgs& a, const TileArgs& t, cudaStream_t st) {
+    constexpr size_t smem = tile_warp_bytes<S>() * kTileWarps;
     static std::mutex mu;
     static std::map<int, unsigned> waves;  // per device: blocks of one resident wave
     int dev = 0;
@@ -760,19 +765,34 @@ egt_status tile_launch(const KnnArgs& a, const TileArgs& t, cudaStream_t st) {
         if (it != waves.end()) G = it->second;
     }
     if (!G) {
-        EGT_CUDA_TRY(cudaFuncSetAttribute(k_knn_tile<kBatch>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)kTileSmem));
+        EGT_CUDA_TRY(cudaFuncSetAttribute(k_knn_tile<kBatch, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
         int sms = 0, per = 0;
         EGT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        EGT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_knn_tile<kBatch>, kTileWarps * 32,
-                                                                    kTileSmem));
+        EGT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_knn_tile<kBatch, S>, kTileWarps * 32,
+                                                                    smem));
         G = (unsigned)std::max(1, sms * std::max(per, 1));
         std::lock_guard<std::mutex> lock(mu);
         waves[dev] = G;
     }
-    k_knn_tile<kBatch><<<G, kTileWarps * 32, kTileSmem, st>>>(a, t);
+    k_knn_tile<kBatch, S><<<G, kTileWarps * 32, smem, st>>>(a, t);
     EGT_LAUNCH_CHECK();
     return EGT_OK;
+}
+
+// kmax: the largest k among the queries the tile search takes.
+template <bool kBatch>
+egt_status tile_launch(const KnnArgs& a, const TileArgs& t, int kmax, cudaStream_t st) {
+    const unsigned T = 256;
+    const int64_t npts = t.npts;
+    k_tile_assign<kBatch><<<(unsigned)((npts + T - 1) / T), T, 0, st>>>(a, t);
+    EGT_LAUNCH_CHECK();
+    const unsigned Gu = (unsigned)std::min<int64_t>(4096, (npts + T - 1) / T);
+    k_tile_count<kBatch><<<Gu, T, 0, st>>>(a, t);
+    EGT_LAUNCH_CHECK();
+    k_tile_gather<kBatch><<<Gu, T, 0, st>>>(a, t);
+    EGT_LAUNCH_CHECK();
+    return kmax <= kTileMaxK2 ? tile_kernel_launch<kBatch, 2>(a, t, st) : tile_kernel_launch<kBatch, 3>(a, t, st);
 }
 
 }  // namespace

@@ -151,14 +151,15 @@ def test_select_matches_ring_search(capi, case, k):
 
 
 @pytest.mark.parametrize("case,k", [("sphere", 40), ("sphere", 16), ("superquadrics", 40), ("superquadrics", 24),
-                                    ("clusters", 20), ("clusters", 40), ("dups", 20), ("lattice", 26),
-                                    ("sphere", 10), ("superquadrics", 41)])
+                                    ("superquadrics", 48), ("superquadrics", 64), ("clusters", 20), ("clusters", 40),
+                                    ("clusters", 64), ("dups", 20), ("lattice", 26), ("sphere", 10),
+                                    ("superquadrics", 65)])
 def test_tile_matches_ring_search(capi, case, k):
-    """The cell-tile search (EGT_KNN_TILE, egt_knn's default for 16 <= k <= 40)
+    """The cell-tile search (EGT_KNN_TILE, egt_knn's default for 16 <= k <= 64)
     against the reference's ring expansion run query by query (EGT_KNN_PLAIN):
     identical lists, invalid rows and deepest level.  Certified rows come from
     the tile kernel, the rest (equal distances, a k-th ball beyond the block,
-    blocks too large or too sparse) from the ring search; k outside [16, 40]
+    blocks too large or too sparse) from the ring search; k outside [16, 64]
     runs the ring search alone."""
     xyz = _cloud_case(case)
     g = cloud(capi, xyz, k)  # the default configuration
@@ -169,7 +170,7 @@ def test_tile_matches_ring_search(capi, case, k):
     assert t["invalid_queries"] == tr["invalid_queries"]
     assert t["levels_used"] == tr["levels_used"]
     n = xyz.shape[0]
-    if not 16 <= k <= 40:
+    if not 16 <= k <= 64:
         assert t["knn_fallback"] == 0 and t["knn_evaluations"] == tr["knn_evaluations"]
     elif case in ("sphere", "superquadrics"):
         assert t["knn_fallback"] < 0.15 * n, t["knn_fallback"]
