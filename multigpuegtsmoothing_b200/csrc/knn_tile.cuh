@@ -59,6 +59,7 @@ constexpr int kTileSparse = 2;       // a finer block below (k+1)/kTileSparse po
                                       // on 4M superquadrics at k = 40: (k+1)/2 and 0.6(k+1) best, 0.75(k+1)
                                       // 8 % slower, 0.45(k+1) and below 15 % slower: its long searches return)
 constexpr int kTileMaxBlock = 6144;   // larger blocks: the ring search (one warp would hold the search's end)
+constexpr int kTileStartLevel = 3;   // the assignment's first level (the usual one on dense clouds)
 constexpr int kTileClasses = 6;       // batch classes by block size (>= 4096, 2048, 1024, 512, 256, less)
 
 struct TileArgs {
@@ -179,8 +180,10 @@ __global__ void __launch_bounds__(256) k_tile_assign(KnnArgs a, TileArgs t) {
         const int thr = kTileAlpha * (A.k + 1), sparse = (A.k + 1) / kTileSparse;
         const uint32_t c0 = __float_as_uint(A.p4[q].w);
         const int cx0 = c0 & 1023u, cy0 = (c0 >> 10) & 1023u, cz0 = (c0 >> 20) & 1023u;
-        int prev = INT_MAX;  // population of the block one level finer
-        for (int l = 0; l < kMaxLevels && lsel < 0; l++) {
+        // Population of the block of level l around the query's cell; the
+        // blocks are nested, so it grows with l, and the first level that
+        // reaches thr is found from a start near the usual one.
+        auto block_pop = [&](int l) {
             const LevelDev& LV = A.lv[l];
             const int cx = cx0 >> l, cy = cy0 >> l, cz = cz0 >> l;
             int pop = 0;
@@ -189,14 +192,28 @@ __global__ void __launch_bounds__(256) k_tile_assign(KnnArgs a, TileArgs t) {
                 const int2 g = row_points(LV, cx - 1, cx + 1, cy + r % 3 - 1, cz + r / 3 - 1);
                 pop += g.y - g.x;
             }
-            if (pop >= thr) {
-                // kMaxLevels: a block too large, or a query alone in its finer
-                // block -- the ring search (such a query's k nearest lie far
-                // off, beyond the block, and its search climbs high)
-                lsel = pop <= t.maxblock && prev >= sparse ? l : kMaxLevels;
-                if (lsel == l) ci = cell_index(LV, cx, cy, cz);
+            return pop;
+        };
+        int l = kTileStartLevel, pop = block_pop(l), prev = INT_MAX;  // prev: the block one level finer
+        if (pop >= thr) {
+            while (l > 0) {
+                const int below = block_pop(l - 1);
+                if (below < thr) { prev = below; break; }
+                l--;
+                pop = below;
             }
-            prev = pop;
+        } else {
+            while (l + 1 < kMaxLevels && pop < thr) {
+                prev = pop;
+                pop = block_pop(++l);
+            }
+        }
+        if (pop >= thr) {
+            // kMaxLevels: a block too large, or a query alone in its finer
+            // block -- the ring search (such a query's k nearest lie far
+            // off, beyond the block, and its search climbs high)
+            lsel = pop <= t.maxblock && prev >= sparse ? l : kMaxLevels;
+            if (lsel == l) ci = cell_index(A.lv[l], cx0 >> l, cy0 >> l, cz0 >> l);
         }
     }
     if (lsel >= kMaxLevels || ci < 0) lsel = -1;  // ci < 0 cannot happen: the query's own cell is occupied
