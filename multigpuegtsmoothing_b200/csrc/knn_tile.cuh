@@ -397,16 +397,20 @@ struct TileUnit {
     const int* order;
     uint32_t lo;   // float bits of the lower edge of bucket 1 less one bucket
     int l;         // level; -1 = no unit
+    // the block's ranges r < seq.m: pref[r] = inclusive prefix end of range r
+    // (INT_MAX past the last), adj[r] = its start less the positions before it
+    int pref[8], adj[9];
 };
 
-// Point index of block position `pos` of a half's unit: the ranges of the
-// unit's block (their inclusive prefix ends and starts, as range_seq16 left
-// them in the half's scratch) are searched for the one holding it.
-__device__ __forceinline__ int tile_point(int pos, const TileUnit& U, const int* s_pref, const int* s_start) {
-    int r = 0;
+// Point index of block position `pos` of a half's unit: position pos lies in
+// range r, the number of ranges ending at or before it, and its level-order
+// slot is pos + adj[r] (the prefix ends increase, so the last test that holds
+// picks r).
+__device__ __forceinline__ int tile_point(int pos, const TileUnit& U) {
+    int a = U.adj[0];
 #pragma unroll
-    for (int t = 0; t < 9; t++) r += (t < U.seq.m && s_pref[t] <= pos) ? 1 : 0;
-    const int local = s_start[r] + (pos - (r > 0 ? s_pref[r - 1] : 0));
+    for (int t = 0; t < 8; t++) a = pos >= U.pref[t] ? U.adj[t + 1] : a;
+    const int local = pos + a;
     return U.order ? __ldg(U.order + local) : local;
 }
 
@@ -460,6 +464,15 @@ __device__ __forceinline__ void tile_unit_setup(const KnnArgs& a, const NormPara
         U.seq = seq;
         U.order = order;
         U.l = l;
+        int before = 0;  // positions of the ranges before range t
+#pragma unroll
+        for (int t = 0; t < 9; t++) {
+            const bool in = t < seq.m;
+            const int end = in ? s_pref[t] : INT_MAX;
+            U.adj[t] = in ? s_start[t] - before : 0;
+            if (t < 8) U.pref[t] = end;
+            if (in) before = end;
+        }
         // buckets: 8 per octave of d^2, bucket 0 below (h/4)^2 and 1/8 octave,
         // bucket kTileBins-1 from 16 h^2 up
         const float h = __fmul_rn(__fsub_rn(np.b, np.a), (float)(1 << l) * (1.0f / 1024.0f));
@@ -470,7 +483,7 @@ __device__ __forceinline__ void tile_unit_setup(const KnnArgs& a, const NormPara
 // Persistent: each half-warp claims batches (up to 16 queries of one unit)
 // one at a time; both halves run their batches together.
 template <bool kBatch, int S>
-__global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArgs t) {
+__global__ void __launch_bounds__(kTileWarps * 32, 16) k_knn_tile(KnnArgs a, TileArgs t) {
     constexpr int kCap = tile_cap<S>();
     constexpr size_t kWarpBytes = tile_warp_bytes<S>();
     extern __shared__ __align__(16) unsigned char s_tile[];
@@ -533,6 +546,11 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
     U.order = nullptr;
     U.lo = 0u;
     U.l = -1;
+#pragma unroll
+    for (int t = 0; t < 9; t++) {
+        U.adj[t] = 0;
+        if (t < 8) U.pref[t] = INT_MAX;
+    }
     unsigned long long n_batches = 0;
 #pragma unroll
     for (int c = 0; c < kTileClasses; c++) n_batches += t.cls_n[c];
@@ -608,7 +626,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
             // the kept candidates' distances, into the bucket space (its offsets are spent)
 #pragma unroll 4
             for (int i = 0; i < m; i++) {
-                const float4 v = __ldg(p4 + tile_point(bpos[tile_slot(i, lane)], U, s_pref, s_start));
+                const float4 v = __ldg(p4 + tile_point(bpos[tile_slot(i, lane)], U));
                 hcol[i * 32] = __float_as_uint(fs_dist3(pq.x, pq.y, pq.z, v.x, v.y, v.z));
             }
             // sorted by (distance, block position); only candidates of one bucket are out of order
@@ -626,7 +644,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
                 bpos[tile_slot(j, lane)] = (uint16_t)ei;
             }
             // the query sits among the distance-0 entries at the front
-            while (self < m - 1 && tile_point(bpos[tile_slot(self, lane)], U, s_pref, s_start) != q) self++;
+            while (self < m - 1 && tile_point(bpos[tile_slot(self, lane)], U) != q) self++;
             // (1) the k+1 smallest distances pairwise distinct
             uint32_t prev = hcol[(self == 0 ? 1 : 0) * 32];
             for (int i = 1; i <= k && ok; i++) {
@@ -666,7 +684,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
                 }
                 if (!ball_in_box(np, pq, kth, lo3, end3)) {
                     for (int i = 0; i < k && ok; i++) {
-                        const int p = tile_point(bpos[tile_slot(i + (i >= self), lane)], U, s_pref, s_start);
+                        const int p = tile_point(bpos[tile_slot(i + (i >= self), lane)], U);
                         ok = visit_step(__float_as_uint(p4[p].w), c0) <= sf;
                     }
                 }
@@ -679,7 +697,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_knn_tile(KnnArgs a, TileArg
         }
         if (ok) {
             int* row = A.lists + (size_t)q * k;
-            for (int i = 0; i < k; i++) row[i] = tile_point(bpos[tile_slot(i + (i >= self), lane)], U, s_pref, s_start);
+            for (int i = 0; i < k; i++) row[i] = tile_point(bpos[tile_slot(i + (i >= self), lane)], U);
             if (A.kth_out) A.kth_out[q] = kth;
             if (A.qlevel) A.qlevel[q] = (uint8_t)reached;
             if constexpr (kBatch) {
