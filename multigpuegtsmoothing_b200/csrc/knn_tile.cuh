@@ -441,6 +441,36 @@ __device__ __forceinline__ void tile_stream16(const TileUnit& U, bool live, int 
     __syncwarp();
 }
 
+// The same stream over a sequence of steps of each half's own: s0 its first
+// step, nxt(s) the step after s (a value >= end: none left).  The warp runs
+// until both halves are done; a half that is done stages padding.
+template <typename N, typename F>
+__device__ __forceinline__ void tile_stream16_seq(const TileUnit& U, int s0, int end, N&& nxt,
+                                                  const float4* __restrict__ p4, float4* chunk, int hl, int hf,
+                                                  F&& f) {
+    const float4 far = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+    int s1 = nxt(s0), s2 = nxt(s1);
+    int pB = seq_index16(U.seq, min(s0, end) * 16, hl, hf, U.order);
+    int pA = seq_index16(U.seq, min(s1, end) * 16, hl, hf, U.order);
+    if (s0 >= end) pB = -1;
+    if (s1 >= end) pA = -1;
+    float4 vB = pB >= 0 ? __ldg(p4 + pB) : far;
+    while (__any_sync(0xffffffffu, s0 < end)) {
+        __syncwarp();
+        chunk[hl] = make_float4(vB.x, vB.y, vB.z, __int_as_float(pB));
+        __syncwarp();
+        pB = pA;
+        vB = pB >= 0 ? __ldg(p4 + pB) : far;
+        pA = seq_index16(U.seq, min(s2, end) * 16, hl, hf, U.order);
+        if (s2 >= end) pA = -1;
+        f(s0);
+        s0 = s1;
+        s1 = s2;
+        s2 = nxt(s2);
+    }
+    __syncwarp();
+}
+
 // Sets up a new unit for the lanes with `take` (both halves call it; a half
 // with take = false keeps its unit).
 __device__ __forceinline__ void tile_unit_setup(const KnnArgs& a, const NormParams& np, int l, int ci, bool take,
@@ -577,8 +607,20 @@ __global__ void __launch_bounds__(kTileWarps * 32, 16) k_knn_tile(KnnArgs a, Til
         const int total = take ? U.seq.total : 0;
         const int steps = (max(total, __shfl_xor_sync(0xffffffffu, total, 16)) + 15) >> 4;
         const uint32_t lo = U.lo;
+        // The smallest bucket of each group of g steps over the half's lanes
+        // (one byte per group in the half's scratch, which the unit set-up no
+        // longer needs): pass 2 visits only the groups that can hold a
+        // candidate it keeps.  2^gs steps per byte (128 bytes cover a block
+        // of up to 8192 candidates).
+        const unsigned hmask = hf ? 0xffff0000u : 0x0000ffffu;
+        const int steps_h = (total + 15) >> 4;
+        const int gs = steps_h > 256 ? 2 : steps_h > 128 ? 1 : 0;
+        uint8_t* mb = reinterpret_cast<uint8_t*>(s_pref);
+        s_pref[hl] = -1;
+        s_pref[hl + 16] = -1;
+        __syncwarp();
         // pass 1: bucket counts (the query itself included, at distance 0)
-        tile_stream16(U, take, steps, p4, chunk, hl, hf, [&](int) {
+        tile_stream16(U, take, steps, p4, chunk, hl, hf, [&](int st) {
             uint32_t bk[16];
 #pragma unroll
             for (int j = 0; j < 16; j++) {
@@ -587,6 +629,14 @@ __global__ void __launch_bounds__(kTileWarps * 32, 16) k_knn_tile(KnnArgs a, Til
             }
 #pragma unroll
             for (int j = 0; j < 16; j++) atomicAdd(hcol + bk[j] * 32, 1u);
+            uint32_t mn = bk[0];
+#pragma unroll
+            for (int j = 1; j < 16; j++) mn = min(mn, bk[j]);
+            mn = __reduce_min_sync(hmask, mn);
+            if (hl == 0 && st < steps_h) {
+                const int gi = st >> gs;
+                mb[gi] = (uint8_t)min((uint32_t)mb[gi], mn);
+            }
         });
         // bucket offsets and the bucket b* of the (k+1)-th distance other
         // than the query's own
@@ -600,8 +650,19 @@ __global__ void __launch_bounds__(kTileWarps * 32, 16) k_knn_tile(KnnArgs a, Til
         }
         bool ok = act && bstar >= 0 && bstar < kTileBins - 1 && m <= kCap;
         const float T = ok ? __uint_as_float(lo + ((uint32_t)(bstar + 1) << 20)) : 0.0f;
-        // pass 2: the candidates of buckets <= b*, in bucket order
-        tile_stream16(U, take, steps, p4, chunk, hl, hf, [&](int st) {
+        // pass 2: the candidates of buckets <= b*, in bucket order, from the
+        // step groups whose smallest bucket is at most the half's largest b*
+        const int bmax = __reduce_max_sync(hmask, ok ? bstar : -1);
+        auto nxt = [&](int st) {
+            int u = st + 1;
+            while (u < steps_h) {
+                const int gi = u >> gs;
+                if ((int)mb[gi] <= bmax) break;
+                u = (gi + 1) << gs;
+            }
+            return min(u, steps_h);
+        };
+        tile_stream16_seq(U, nxt(-1), steps_h, nxt, p4, chunk, hl, hf, [&](int st) {
 #pragma unroll
             for (int j0 = 0; j0 < 16; j0 += 8) {
                 float dd[8];
