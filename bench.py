@@ -520,6 +520,10 @@ def run_b200(args, world, rank, local):
         g.GRIDCUDAKNNSELF_COMPACT(K)
         ev[i][2].record(stream)
     t1.record(stream)
+    # wait with short sleeps, so that the clock sampler's thread runs while
+    # the timed steps execute (a blocking synchronize gives it no turn)
+    while not t1.query():
+        time.sleep(0.0005)
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()
