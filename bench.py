@@ -126,21 +126,26 @@ class ClockSampler:
         except OSError:
             self.p = None
 
-    def _sample(self):
+    def _sample(self, with_max: bool = False):
+        # the maximum clock is a constant: read at the start and the end only
+        # (each NVML query can take milliseconds)
         nv = self.nvml
         self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
-        self.smax.append(float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)))
+        if with_max:
+            self.smax.append(float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)))
         active = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
         for nm, m in zip(self.NAMES, self.masks):
             if active & m:
                 self.reasons.add(nm)
 
     def _poll(self):
+        first = True
         while True:
             try:
-                self._sample()
+                self._sample(with_max=first)
             except Exception:
                 return
+            first = False
             if self.stop_flag.wait(0.01):
                 return
 
@@ -149,7 +154,7 @@ class ClockSampler:
             self.stop_flag.set()
             self.thread.join()
             try:
-                self._sample()  # at least one sample at the end of the region
+                self._sample(with_max=True)  # at least one sample at the end of the region
             except Exception:
                 pass
             try:
