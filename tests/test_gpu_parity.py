@@ -119,6 +119,12 @@ def _cloud_case(case):
     if case == "clusters":
         return np.concatenate([rng.normal(c, s, (20000, 3)) for c, s in
                                [((0, 0, 0), 0.002), ((0.5, 0.1, 0), 0.05), ((1, 1, 1), 0.3)]]).astype(np.float32)
+    if case == "halo":
+        # a dense ball in a sparse cube: near the ball, the level a background
+        # query's block first reaches the selecting population also takes in
+        # thousands of the ball's points (blocks of 2,048-6,144 candidates,
+        # the tile kernel's coarser step groups)
+        return np.concatenate([rng.normal(0.5, 0.01, (40000, 3)), rng.random((40000, 3))]).astype(np.float32)
     d, _ = load("ref_lattice" if case == "lattice" else "ref_dups")
     return d["in_xyz"]
 
@@ -152,8 +158,8 @@ def test_select_matches_ring_search(capi, case, k):
 
 @pytest.mark.parametrize("case,k", [("sphere", 40), ("sphere", 16), ("superquadrics", 40), ("superquadrics", 24),
                                     ("superquadrics", 48), ("superquadrics", 64), ("clusters", 20), ("clusters", 40),
-                                    ("clusters", 64), ("dups", 20), ("lattice", 26), ("sphere", 10),
-                                    ("superquadrics", 65)])
+                                    ("clusters", 64), ("halo", 40), ("halo", 64), ("dups", 20), ("lattice", 26),
+                                    ("sphere", 10), ("superquadrics", 65)])
 def test_tile_matches_ring_search(capi, case, k):
     """The cell-tile search (EGT_KNN_TILE, egt_knn's default for 16 <= k <= 64)
     against the reference's ring expansion run query by query (EGT_KNN_PLAIN):
@@ -174,7 +180,7 @@ def test_tile_matches_ring_search(capi, case, k):
         assert t["knn_fallback"] == 0 and t["knn_evaluations"] == tr["knn_evaluations"]
     elif case in ("sphere", "superquadrics"):
         assert t["knn_fallback"] < 0.15 * n, t["knn_fallback"]
-    elif case == "clusters":
+    elif case in ("clusters", "halo"):
         # the densest cluster's level-0 blocks exceed the tile cap: ring search
         assert t["knn_fallback"] < 0.5 * n, t["knn_fallback"]
     elif case == "lattice":
