@@ -13,12 +13,14 @@
 //
 //   pass 1  each lane buckets its candidate distances (64 buckets, 8 per
 //           octave of d^2 from (h/4)^2 to (4h)^2, h the level's cell side)
-//           and finds the bucket b* holding its (k+1)-th smallest;
+//           and finds the bucket b* holding its (k+1)-th smallest; the half
+//           records the smallest bucket of each group of steps;
 //   pass 2  each lane keeps the block positions (16 bits) of buckets <= b*
-//           (at most tile_cap) in bucket order (offsets from pass 1's counts);
-//           their distances are computed again into the spent bucket space
-//           and the list is insertion-sorted (only candidates of one bucket
-//           are out of order).
+//           (at most tile_cap) in bucket order (offsets from pass 1's counts),
+//           visiting only the step groups whose smallest bucket is at most
+//           the half's largest b*; the kept distances are computed again into
+//           the spent bucket space and the list is insertion-sorted (only
+//           candidates of one bucket are out of order).
 //
 // The result is accepted only when it provably equals the ring search's list
 // (the conditions of the proposal-driven box search, knn.cu): the k+1
@@ -120,7 +122,8 @@ constexpr size_t tile_warp_bytes() {
     return (size_t)tile_rows<S>() * 32 * 4         // bucket counts, offsets, then kept distances [row][lane]
            + (size_t)tile_cap<S>() * 32 * 2        // kept candidates' block positions [slot][lane]
            + 2 * 16 * 16                           // staged candidates per half (x, y, z, point)
-           + 2 * 2 * 16 * 4;                       // range sequence scratch per half
+           + 2 * 2 * 16 * 4;                       // per half: range sequence scratch at unit set-up,
+                                                   // then the step groups' smallest buckets
 }
 
 // Kept-candidate slot s of lane `lane` (16-bit entries: two lanes per bank word).
